@@ -1,0 +1,183 @@
+/*
+ * parbutterfly_b200 — C ABI of the B200-native butterfly counting / peeling library.
+ *
+ * The reference (ParButterfly, apps/hyper/) has no FFI: its boundary is the
+ * BipartiteButterflies CLI and the C++ entry points that Compute() calls
+ * (apps/hyper/BipartiteButterflies.C:75-277).  Every entry point below replaces one of
+ * those calls; the comment on each one cites the reference function it stands in for.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Graph arrays use the reference's default integer
+ *    widths: offsets are uintT (uint32_t) and vertex ids are uintE (uint32_t)
+ *    (ligra/parallel.h:102-125, no -DLONG / -DEDGELONG).  Counts are int64_t ("long").
+ *  - Outputs are DENSE int64 arrays (the reference strides them by 8 longs, one per cache
+ *    line, e.g. BipartiteButterflies.C:228-232; the stride carries no information and is
+ *    dropped).  Output pointers may be host or device memory; the library detects which.
+ *  - Every call returns a pb_status and never exits the process (the reference prints and
+ *    calls exit(0)/abort(), e.g. butterfly_utils.h:1014-1016,1040,1050).  On error,
+ *    pb_last_error() returns a message for the calling context.
+ *  - All calls are synchronous with respect to the context's CUDA stream on return.
+ *  - One pb_ctx per host thread; distinct contexts are independent.
+ */
+#ifndef PARBUTTERFLY_B200_H
+#define PARBUTTERFLY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_ABI_VERSION 1
+
+typedef enum {
+  PB_OK = 0,
+  PB_EINVAL = 1,       /* bad argument or malformed CSR (unsorted list, id out of range, mv != mu) */
+  PB_ENOMEM = 2,       /* device or host allocation failed */
+  PB_ETOOBIG = 3,      /* a size exceeds a documented limit */
+  PB_ETIMEOUT = 4,     /* a bounded device wait ran out; the context stays usable */
+  PB_ECUDA = 5,        /* a CUDA runtime call failed */
+  PB_EUNSUPPORTED = 6, /* option outside the supported surface (e.g. sparsification) */
+  PB_EIO = 7           /* file could not be read / parsed */
+} pb_status;
+
+/* Enum values and order follow apps/hyper/butterfly_utils.h:24-28 exactly. */
+typedef enum { PB_SORT = 0, PB_ASORT, PB_HASH, PB_AHASH, PB_HIST, PB_AHIST, PB_BATCHS, PB_BATCHWA, PB_SERIAL } pb_count_type;
+typedef enum { PB_SIDE = 0, PB_COCORE, PB_ACOCORE, PB_DEG, PB_ADEG } pb_rank_type;
+typedef enum { PB_PSORT = 0, PB_PHASH, PB_PHIST, PB_PBATCHS, PB_PBATCHWA } pb_peel_type;
+typedef enum { PB_VERT = 0, PB_EDGE, PB_TOTAL } pb_per_type;
+
+/* Strategy scheduler: PLAIN = the fixed strategy named by count_type; LEARNED = per-block
+ * strategy picked by the learned scheduler (results are identical either way). */
+typedef enum { PB_SCHED_PLAIN = 0, PB_SCHED_LEARNED = 1 } pb_sched;
+
+/* Options.  Field meanings and defaults follow the CLI of BipartiteButterflies.C:79-194. */
+typedef struct {
+  int32_t count_type;     /* pb_count_type, default PB_SERIAL (BipartiteButterflies.C:92) */
+  int32_t rank_type;      /* pb_rank_type, default PB_ADEG (BipartiteButterflies.C:118) */
+  int32_t peel_type;      /* pb_peel_type, default PB_PBATCHS */
+  int32_t per_type;       /* pb_per_type, default PB_VERT */
+  int64_t max_wedges;     /* -m, default 2577500000 (BipartiteButterflies.C:172) */
+  int64_t max_array_size; /* -a, default 23090996160 (BipartiteButterflies.C:173) */
+  int32_t sched;          /* pb_sched, default PB_SCHED_PLAIN */
+  int32_t autotune;       /* 0/1: let the autotuner pick tile/batch/table sizes */
+  int32_t use_v;          /* -1 = choose as cmpWedgeCounts does; 0/1 forces the count side */
+  int32_t reserved;
+} pb_opts;
+
+/* Host-side two-sided CSR, the layout of struct bipartiteCSR (butterfly_utils.h:184-197).
+ * offsetsV[nv+1], edgesV[m] (U ids), offsetsU[nu+1], edgesU[m] (V ids); every adjacency
+ * list sorted ascending without duplicates (the contract of utils/graphIO.h:378-420). */
+typedef struct {
+  int64_t nv, nu, m;
+  const uint32_t* offsetsV;
+  const uint32_t* edgesV;
+  const uint32_t* offsetsU;
+  const uint32_t* edgesU;
+} pb_csr;
+
+/* Owned host CSR returned by the generators and the file reader; release with pb_csr_free. */
+typedef struct {
+  int64_t nv, nu, m;
+  uint32_t* offsetsV;
+  uint32_t* edgesV;
+  uint32_t* offsetsU;
+  uint32_t* edgesU;
+} pb_csr_owned;
+
+/* Per-call statistics of the last count/peel call on a context. */
+typedef struct {
+  int64_t w_side;         /* get<1>(cmpWedgeCounts(G)) (butterfly_utils.h:1080-1086) */
+  int64_t w_rank;         /* wedges the ranked traversal enumerates (countWedgesScan total) */
+  int32_t use_v;          /* count side actually used */
+  int32_t n_big;          /* endpoints handled by the block-cooperative aggregator */
+  double ms_rank;         /* ranking: vertex order (ADEG/DEG/COCORE/ACOCORE/SIDE) */
+  double ms_relabel;      /* ranked CSR build (rankGraph / rankGraphEdges) */
+  double ms_scan;         /* wedge scan (countWedgesScan) */
+  double ms_count;        /* wedge aggregation + butterfly accumulation */
+  double ms_convert;      /* rank -> original index conversion */
+  double ms_peel;         /* peeling (tip or wing) */
+  int64_t peel_rounds;    /* bucket rounds executed by the last peel call */
+  int64_t peel_work;      /* wedges (tip) or intersection probes (wing) processed while peeling */
+  double ms_agg_kernel;   /* device time of the aggregation kernels alone */
+} pb_stats;
+
+typedef struct pb_ctx pb_ctx;
+typedef struct pb_graph pb_graph;
+
+/* ---- library / context ---------------------------------------------------------------- */
+int pb_abi_version(void);
+void pb_opts_default(pb_opts* opts);
+/* Creates a context on CUDA device `device`.  `stream` is a cudaStream_t or NULL (the context
+ * then creates its own non-blocking stream). */
+pb_status pb_ctx_create(int device, void* stream, pb_ctx** out);
+pb_status pb_ctx_destroy(pb_ctx* ctx);
+const char* pb_last_error(const pb_ctx* ctx);
+pb_status pb_get_stats(const pb_ctx* ctx, pb_stats* out);
+/* Counts of this library's kernel launches on the context since creation (for reporting). */
+int64_t pb_kernel_launches(const pb_ctx* ctx);
+
+/* ---- graph ----------------------------------------------------------------------------- */
+/* Copies a host CSR to the device and validates it (sortedness, ranges, mv == mu); replaces
+ * the in-memory result of readBipartite (butterfly_utils.h:1008-1058). */
+pb_status pb_graph_upload(pb_ctx* ctx, const pb_csr* host, pb_graph** out);
+/* Same contract, for arrays already resident in device memory (copied, not adopted). */
+pb_status pb_graph_from_device(pb_ctx* ctx, const pb_csr* dev, pb_graph** out);
+pb_status pb_graph_destroy(pb_graph* g);
+pb_status pb_graph_dims(const pb_graph* g, int64_t* nv, int64_t* nu, int64_t* m);
+
+/* cmpWedgeCounts (butterfly_utils.h:1080-1086): *use_v = (W_V <= W_U), *num_wedges = min. */
+pb_status pb_cmp_wedge_counts(pb_ctx* ctx, const pb_graph* g, int32_t* use_v, int64_t* num_wedges);
+
+/* edgeToIdxs (butterfly_utils.h:2034-2062): eti[m], for the orientation given by use_v. */
+pb_status pb_edge_to_idxs(pb_ctx* ctx, const pb_graph* g, int32_t use_v, uint32_t* eti);
+
+/* ---- counting -------------------------------------------------------------------------- */
+/* Count (butterfly_count.h:1634-1731): out[nCount] per count-side vertex, original ids;
+ * nCount = nu if use_v else nv. */
+pb_status pb_count_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out);
+/* CountE (butterfly_ecount.h:1766-1899): out[m] per edge, indexed like the reference's
+ * result: by position in edgesV when use_v, else by position in edgesU. */
+pb_status pb_count_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out);
+/* CountTotal (butterfly_count_total.h:1014-1102): total number of butterflies. */
+pb_status pb_count_total(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out);
+
+/* ---- peeling --------------------------------------------------------------------------- */
+/* Peel (butterfly_peel.h:896-934): tip numbers tip[nCount] from per-vertex counts (as from
+ * pb_count_vert with the same use_v).  64-bit buckets throughout. */
+pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* counts,
+                       int64_t* tip);
+/* PeelE (butterfly_epeel.h:519-569): wing numbers wing[m] from per-edge counts (edge order of
+ * pb_count_edge).  The graph is not modified (the reference tombstones its input). */
+pb_status pb_peel_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* ecounts,
+                       int64_t* wing);
+
+/* ---- host utilities (no GPU needed) ---------------------------------------------------- */
+void pb_csr_free(pb_csr_owned* g);
+/* readBipartite (butterfly_utils.h:1008-1058): Ligra "AdjacencyHypergraph" text file. */
+pb_status pb_read_adjacency_hypergraph(const char* path, pb_csr_owned* out);
+/* Writer for the same format (utils/graphIO.h:752-779 layout). */
+pb_status pb_write_adjacency_hypergraph(const char* path, const pb_csr* g);
+/* Host validation of a CSR (same checks as pb_graph_upload). */
+pb_status pb_csr_validate(const pb_csr* g, char* msg, size_t msg_len);
+
+/* Seeded generators (SplitMix64 counter RNG).  Each draws edges until m distinct (v,u) pairs
+ * exist and returns both adjacency sides sorted. */
+pb_status pb_gen_uniform(int64_t nv, int64_t nu, int64_t m, uint64_t seed, pb_csr_owned* out);
+/* Bipartite R-MAT on a 2^log_nv x 2^log_nu grid with quadrant probabilities a,b,c,d. */
+pb_status pb_gen_rmat(int32_t log_nv, int32_t log_nu, int64_t m, double a, double b, double c, double d,
+                      uint64_t seed, pb_csr_owned* out);
+/* U side with discrete power-law degrees p(k) ~ k^-alpha on [dmin, dmax] (sum trimmed to m),
+ * each U vertex joined to distinct uniform V vertices. */
+pb_status pb_gen_powerlaw_u(int64_t nv, int64_t nu, int64_t m, double alpha, int64_t dmax, uint64_t seed,
+                            pb_csr_owned* out);
+/* Endpoints drawn with Zipf(s) over ids on both sides (s = 0 gives uniform). */
+pb_status pb_gen_zipf(int64_t nv, int64_t nu, int64_t m, double s, uint64_t seed, pb_csr_owned* out);
+/* Graph g of the 256-graph batch workload (sizes log-uniform; seed 4000+g). */
+pb_status pb_gen_batch_member(int32_t g, pb_csr_owned* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARBUTTERFLY_B200_H */

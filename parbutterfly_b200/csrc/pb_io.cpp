@@ -1,0 +1,168 @@
+// Host-side input/output for the Ligra AdjacencyHypergraph format and CSR validation.
+//
+// Format (readBipartite, butterfly_utils.h:1008-1058; writer layout utils/graphIO.h:752-779):
+//   AdjacencyHypergraph
+//   nv  mv  nu  mu
+//   offsetsV[0..nv)   edgesV[0..mv)   offsetsU[0..nu)   edgesU[0..mu)
+// whitespace separated.  The reference aborts with "Bad input file" when the header word is
+// wrong, the token count is not nv+mv+nu+mu+5, or mv != mu (:1013-1027), and exits when an
+// edge id is out of range (:1039-1051).  Here each of those is a PB_EINVAL/PB_EIO status.
+#include <cerrno>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/parbutterfly_b200.h"
+
+namespace {
+
+struct Tokenizer {
+  const char* p;
+  const char* end;
+  bool next_word(const char*& s, size_t& len) {
+    while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
+    if (p >= end) return false;
+    s = p;
+    while (p < end && !(*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
+    len = (size_t)(p - s);
+    return true;
+  }
+  bool next_u64(uint64_t& x) {
+    const char* s;
+    size_t len;
+    if (!next_word(s, len)) return false;
+    uint64_t v = 0;
+    for (size_t i = 0; i < len; ++i) {
+      unsigned c = (unsigned)(s[i] - '0');
+      if (c > 9) return false;
+      v = v * 10 + c;
+    }
+    x = v;
+    return true;
+  }
+};
+
+pb_status fill_msg(char* msg, size_t msg_len, pb_status st, const std::string& s) {
+  if (msg && msg_len) {
+    std::snprintf(msg, msg_len, "%s", s.c_str());
+  }
+  return st;
+}
+
+// Checks one side: offsets monotone, ends at m, each list strictly ascending, ids < other_n.
+pb_status check_side(const uint32_t* off, const uint32_t* edg, int64_t n, int64_t m, int64_t other_n,
+                     const char* side, char* msg, size_t msg_len) {
+  if (off[0] != 0) return fill_msg(msg, msg_len, PB_EINVAL, std::string("offsets") + side + "[0] != 0");
+  if ((int64_t)off[n] != m) return fill_msg(msg, msg_len, PB_EINVAL, std::string("offsets") + side + "[n] != m");
+  for (int64_t i = 0; i < n; ++i) {
+    if (off[i + 1] < off[i])
+      return fill_msg(msg, msg_len, PB_EINVAL, std::string("offsets") + side + " not monotone at " + std::to_string(i));
+    for (uint32_t e = off[i]; e < off[i + 1]; ++e) {
+      if ((int64_t)edg[e] >= other_n)
+        return fill_msg(msg, msg_len, PB_EINVAL,
+                        std::string("edges") + side + " out of range: id " + std::to_string(edg[e]) + " at " + std::to_string(e));
+      if (e > off[i] && edg[e] <= edg[e - 1])
+        return fill_msg(msg, msg_len, PB_EINVAL,
+                        std::string("edges") + side + " list of vertex " + std::to_string(i) + " not strictly ascending");
+    }
+  }
+  return PB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pb_status pb_csr_validate(const pb_csr* g, char* msg, size_t msg_len) {
+  if (!g) return fill_msg(msg, msg_len, PB_EINVAL, "null graph");
+  if (g->nv < 0 || g->nu < 0 || g->m < 0) return fill_msg(msg, msg_len, PB_EINVAL, "negative size");
+  if (g->nv > (int64_t)UINT32_MAX / 2 || g->nu > (int64_t)UINT32_MAX / 2 || g->nv + g->nu >= (int64_t)(1u << 31))
+    return fill_msg(msg, msg_len, PB_ETOOBIG, "nv + nu must stay below 2^31 (ranked ids carry a tag bit)");
+  if (2 * g->m > (int64_t)UINT32_MAX) return fill_msg(msg, msg_len, PB_ETOOBIG, "2*m must fit 32-bit offsets");
+  if (!g->offsetsV || !g->offsetsU || (g->m > 0 && (!g->edgesV || !g->edgesU)))
+    return fill_msg(msg, msg_len, PB_EINVAL, "null array");
+  pb_status st = check_side(g->offsetsV, g->edgesV, g->nv, g->m, g->nu, "V", msg, msg_len);
+  if (st != PB_OK) return st;
+  st = check_side(g->offsetsU, g->edgesU, g->nu, g->m, g->nv, "U", msg, msg_len);
+  if (st != PB_OK) return st;
+  // Both sides must describe the same edge set: per-vertex degree agreement is implied by
+  // the transpose check below (count of each (v,u) in V lists equals that in U lists).
+  std::vector<uint32_t> cur(g->offsetsU, g->offsetsU + g->nu);
+  for (int64_t v = 0; v < g->nv; ++v) {
+    for (uint32_t e = g->offsetsV[v]; e < g->offsetsV[v + 1]; ++e) {
+      uint32_t u = g->edgesV[e];
+      if (cur[u] >= g->offsetsU[u + 1] || g->edgesU[cur[u]] != (uint32_t)v)
+        return fill_msg(msg, msg_len, PB_EINVAL, "edgesV and edgesU describe different edge sets");
+      cur[u]++;
+    }
+  }
+  return fill_msg(msg, msg_len, PB_OK, "");
+}
+
+pb_status pb_read_adjacency_hypergraph(const char* path, pb_csr_owned* out) {
+  if (!path || !out) return PB_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return PB_EIO;
+  std::vector<char> buf;
+  if (std::fseek(f, 0, SEEK_END) != 0) { std::fclose(f); return PB_EIO; }
+  long size = std::ftell(f);
+  if (size < 0) { std::fclose(f); return PB_EIO; }
+  std::rewind(f);
+  buf.resize((size_t)size);
+  if (size > 0 && std::fread(buf.data(), 1, (size_t)size, f) != (size_t)size) { std::fclose(f); return PB_EIO; }
+  std::fclose(f);
+  Tokenizer t{buf.data(), buf.data() + buf.size()};
+  const char* w;
+  size_t len;
+  if (!t.next_word(w, len) || std::string(w, len) != "AdjacencyHypergraph") return PB_EINVAL;
+  uint64_t nv, mv, nu, mu;
+  if (!t.next_u64(nv) || !t.next_u64(mv) || !t.next_u64(nu) || !t.next_u64(mu)) return PB_EINVAL;
+  if (mv != mu) return PB_EINVAL;
+  if (nv >= (1ull << 31) || nu >= (1ull << 31) || mv >= (1ull << 32)) return PB_ETOOBIG;
+  pb_csr_owned g;
+  g.nv = (int64_t)nv; g.nu = (int64_t)nu; g.m = (int64_t)mv;
+  g.offsetsV = (uint32_t*)malloc(sizeof(uint32_t) * (nv + 1));
+  g.offsetsU = (uint32_t*)malloc(sizeof(uint32_t) * (nu + 1));
+  g.edgesV = (uint32_t*)malloc(sizeof(uint32_t) * (mv ? mv : 1));
+  g.edgesU = (uint32_t*)malloc(sizeof(uint32_t) * (mu ? mu : 1));
+  if (!g.offsetsV || !g.offsetsU || !g.edgesV || !g.edgesU) { pb_csr_free(&g); return PB_ENOMEM; }
+  auto read_arr = [&](uint32_t* a, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) {
+      uint64_t x;
+      if (!t.next_u64(x) || x > UINT32_MAX) return false;
+      a[i] = (uint32_t)x;
+    }
+    return true;
+  };
+  if (!read_arr(g.offsetsV, nv) || !read_arr(g.edgesV, mv) || !read_arr(g.offsetsU, nu) || !read_arr(g.edgesU, mu)) {
+    pb_csr_free(&g);
+    return PB_EINVAL;
+  }
+  uint64_t extra;
+  if (t.next_u64(extra)) { pb_csr_free(&g); return PB_EINVAL; }  // token count mismatch
+  g.offsetsV[nv] = (uint32_t)mv;
+  g.offsetsU[nu] = (uint32_t)mu;
+  for (uint64_t i = 0; i < mv; ++i) if (g.edgesV[i] >= nu) { pb_csr_free(&g); return PB_EINVAL; }
+  for (uint64_t i = 0; i < mu; ++i) if (g.edgesU[i] >= nv) { pb_csr_free(&g); return PB_EINVAL; }
+  *out = g;
+  return PB_OK;
+}
+
+pb_status pb_write_adjacency_hypergraph(const char* path, const pb_csr* g) {
+  if (!path || !g) return PB_EINVAL;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return PB_EIO;
+  std::fprintf(f, "AdjacencyHypergraph\n%lld\n%lld\n%lld\n%lld\n", (long long)g->nv, (long long)g->m,
+               (long long)g->nu, (long long)g->m);
+  for (int64_t i = 0; i < g->nv; ++i) std::fprintf(f, "%u\n", g->offsetsV[i]);
+  for (int64_t i = 0; i < g->m; ++i) std::fprintf(f, "%u\n", g->edgesV[i]);
+  for (int64_t i = 0; i < g->nu; ++i) std::fprintf(f, "%u\n", g->offsetsU[i]);
+  for (int64_t i = 0; i < g->m; ++i) std::fprintf(f, "%u\n", g->edgesU[i]);
+  return std::fclose(f) == 0 ? PB_OK : PB_EIO;
+}
+
+}  // extern "C"
