@@ -1,0 +1,213 @@
+"""Host-side mirror of ParButterfly's entry points over the C ABI.
+
+Names and argument meanings follow the C++ functions that BipartiteButterflies' Compute()
+calls (apps/hyper/BipartiteButterflies.C:75-277):
+
+  cmp_wedge_counts(G)                -> cmpWedgeCounts   (butterfly_utils.h:1080-1086)
+  edge_to_idxs(G, use_v)             -> edgeToIdxs       (butterfly_utils.h:2034-2062)
+  count(G, count_type, rank_type)    -> Count            (butterfly_count.h:1634-1731)
+  count_e(G, count_type, rank_type)  -> CountE           (butterfly_ecount.h:1766-1899)
+  count_total(G, ...)                -> CountTotal       (butterfly_count_total.h:1014-1102)
+  peel(G, counts, peel_type)         -> Peel             (butterfly_peel.h:896-934)
+  peel_e(G, ecounts, peel_type)      -> PeelE            (butterfly_epeel.h:519-569)
+
+Results are dense int64 numpy arrays (the reference strides its arrays by 8 longs).  Unlike
+the reference, errors raise PBError instead of exiting, and PeelE leaves the graph intact.
+Inputs may be numpy (host) or torch CUDA tensors (device); outputs follow `out=` when given.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+from .graph import BipartiteGraph
+
+COUNT_TYPES = {"SORT": 0, "ASORT": 1, "HASH": 2, "AHASH": 3, "HIST": 4, "AHIST": 5, "BATCHS": 6, "BATCHWA": 7,
+               "SERIAL": 8}
+RANK_TYPES = {"SIDE": 0, "COCORE": 1, "ACOCORE": 2, "DEG": 3, "ADEG": 4}
+PEEL_TYPES = {"SORT": 0, "HASH": 1, "HIST": 2, "BATCHS": 3, "BATCHWA": 4}
+PER_TYPES = {"VERT": 0, "EDGE": 1, "TOTAL": 2}
+
+
+def _enum(table, v, what):
+    if isinstance(v, str):
+        if v not in table:
+            raise ValueError(f"unknown {what} {v!r}; expected one of {sorted(table)}")
+        return table[v]
+    return int(v)
+
+
+def make_opts(count_type="SERIAL", rank_type="ADEG", peel_type="BATCHS", per="VERT", use_v: Optional[bool] = None,
+              max_wedges=2577500000, max_array_size=23090996160, sched="plain", autotune=False) -> _ffi.Opts:
+    o = _ffi.Opts()
+    _ffi.lib().pb_opts_default(C.byref(o))
+    o.count_type = _enum(COUNT_TYPES, count_type, "count type")
+    o.rank_type = _enum(RANK_TYPES, rank_type, "rank type")
+    o.peel_type = _enum(PEEL_TYPES, peel_type, "peel type")
+    o.per_type = _enum(PER_TYPES, per, "per type")
+    o.max_wedges = int(max_wedges)
+    o.max_array_size = int(max_array_size)
+    o.sched = 1 if str(sched).lower() == "learned" else 0
+    o.autotune = 1 if autotune else 0
+    o.use_v = -1 if use_v is None else int(bool(use_v))
+    return o
+
+
+class Context:
+    """A pb_ctx: one CUDA device and stream.  Use one per host thread."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        self._lib = _ffi.lib()
+        self._h = C.c_void_p()
+        _ffi.check(self._lib.pb_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(self._h)),
+                   what="pb_ctx_create")
+        self.device = device
+
+    def close(self):
+        if self._h:
+            self._lib.pb_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, st, what=""):
+        _ffi.check(st, self._h, what)
+
+    def stats(self) -> dict:
+        s = _ffi.Stats()
+        self.check(self._lib.pb_get_stats(self._h, C.byref(s)), "pb_get_stats")
+        return {name: getattr(s, name) for name, _ in _ffi.Stats._fields_}
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.pb_kernel_launches(self._h))
+
+    def upload(self, g: BipartiteGraph) -> "DeviceGraph":
+        return DeviceGraph(self, g)
+
+
+class DeviceGraph:
+    """A pb_graph: the two-sided CSR resident in device memory."""
+
+    def __init__(self, ctx: Context, g: Optional[BipartiteGraph] = None, *, device_arrays=None):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        lib = ctx._lib
+        if g is not None:
+            s = g.csr_struct()
+            ctx.check(lib.pb_graph_upload(ctx.handle, C.byref(s), C.byref(self._h)), "pb_graph_upload")
+            self.nv, self.nu, self.m = g.nv, g.nu, g.m
+        else:
+            nv, nu, offV, edgV, offU, edgU = device_arrays
+            m = int(edgV.numel())
+            s = _ffi.CSR(nv, nu, m, offV.data_ptr(), edgV.data_ptr(), offU.data_ptr(), edgU.data_ptr())
+            ctx.check(lib.pb_graph_from_device(ctx.handle, C.byref(s), C.byref(self._h)), "pb_graph_from_device")
+            self.nv, self.nu, self.m = nv, nu, m
+
+    def close(self):
+        if self._h:
+            self.ctx._lib.pb_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+
+def _ptr(a):
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _out(n, out):
+    if out is not None:
+        return out
+    return np.zeros(max(n, 1), dtype=np.int64)
+
+
+def cmp_wedge_counts(dg: DeviceGraph):
+    uv, w = C.c_int32(), C.c_int64()
+    dg.ctx.check(dg.ctx._lib.pb_cmp_wedge_counts(dg.ctx.handle, dg.handle, C.byref(uv), C.byref(w)),
+                 "pb_cmp_wedge_counts")
+    return bool(uv.value), int(w.value)
+
+
+def edge_to_idxs(dg: DeviceGraph, use_v: bool):
+    eti = np.zeros(max(dg.m, 1), dtype=np.uint32)
+    dg.ctx.check(dg.ctx._lib.pb_edge_to_idxs(dg.ctx.handle, dg.handle, int(use_v), eti.ctypes.data),
+                 "pb_edge_to_idxs")
+    return eti[:dg.m]
+
+
+def count(dg: DeviceGraph, count_type="SERIAL", rank_type="ADEG", use_v=None, out=None, **kw):
+    """Per-vertex butterfly counts of the count side (original vertex ids)."""
+    if use_v is None:
+        use_v = cmp_wedge_counts(dg)[0]
+    n = dg.nu if use_v else dg.nv
+    res = _out(n, out)
+    o = make_opts(count_type, rank_type, per="VERT", use_v=use_v, **kw)
+    dg.ctx.check(dg.ctx._lib.pb_count_vert(dg.ctx.handle, dg.handle, C.byref(o), _ptr(res)), "pb_count_vert")
+    return res[:n] if out is None else res
+
+
+def count_e(dg: DeviceGraph, count_type="SERIAL", rank_type="ADEG", use_v=None, out=None, **kw):
+    """Per-edge butterfly counts, indexed like the reference's CountE result."""
+    if use_v is None:
+        use_v = cmp_wedge_counts(dg)[0]
+    res = _out(dg.m, out)
+    o = make_opts(count_type, rank_type, per="EDGE", use_v=use_v, **kw)
+    dg.ctx.check(dg.ctx._lib.pb_count_edge(dg.ctx.handle, dg.handle, C.byref(o), _ptr(res)), "pb_count_edge")
+    return res[:dg.m] if out is None else res
+
+
+def count_total(dg: DeviceGraph, count_type="SERIAL", rank_type="ADEG", use_v=None, **kw) -> int:
+    res = np.zeros(1, dtype=np.int64)
+    o = make_opts(count_type, rank_type, per="TOTAL", use_v=use_v, **kw)
+    dg.ctx.check(dg.ctx._lib.pb_count_total(dg.ctx.handle, dg.handle, C.byref(o), res.ctypes.data), "pb_count_total")
+    return int(res[0])
+
+
+def peel(dg: DeviceGraph, counts, peel_type="BATCHS", use_v=None, out=None, **kw):
+    """Tip numbers from per-vertex counts."""
+    if use_v is None:
+        use_v = cmp_wedge_counts(dg)[0]
+    n = dg.nu if use_v else dg.nv
+    c = counts if not isinstance(counts, np.ndarray) else np.ascontiguousarray(counts, dtype=np.int64)
+    res = _out(n, out)
+    o = make_opts(peel_type=peel_type, per="VERT", use_v=use_v, **kw)
+    dg.ctx.check(dg.ctx._lib.pb_peel_vert(dg.ctx.handle, dg.handle, C.byref(o), _ptr(c), _ptr(res)), "pb_peel_vert")
+    return res[:n] if out is None else res
+
+
+def peel_e(dg: DeviceGraph, ecounts, peel_type="BATCHS", use_v=None, out=None, **kw):
+    """Wing numbers from per-edge counts."""
+    if use_v is None:
+        use_v = cmp_wedge_counts(dg)[0]
+    c = ecounts if not isinstance(ecounts, np.ndarray) else np.ascontiguousarray(ecounts, dtype=np.int64)
+    res = _out(dg.m, out)
+    o = make_opts(peel_type=peel_type, per="EDGE", use_v=use_v, **kw)
+    dg.ctx.check(dg.ctx._lib.pb_peel_edge(dg.ctx.handle, dg.handle, C.byref(o), _ptr(c), _ptr(res)), "pb_peel_edge")
+    return res[:dg.m] if out is None else res

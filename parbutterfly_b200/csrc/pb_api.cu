@@ -1,0 +1,531 @@
+// C ABI of libpbgpu: contexts, graphs and the Count / CountE / CountTotal / Peel / PeelE
+// entry points (include/parbutterfly_b200.h).
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pb_engine.cuh"
+#include "pb_prims.cuh"
+
+struct pb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  pb_stats stats{};
+  int64_t launches = 0;
+};
+
+namespace pb {
+
+thread_local int64_t* g_launch_counter = nullptr;
+
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+namespace {
+
+// Sets the device and the launch counter of a context for the duration of one API call.
+struct CallScope {
+  pb_ctx* ctx;
+  int prev_dev = -1;
+  explicit CallScope(pb_ctx* c) : ctx(c) {
+    cudaGetDevice(&prev_dev);
+    if (prev_dev != c->device) PB_CUDA_TRY(cudaSetDevice(c->device));
+    g_launch_counter = &c->launches;
+  }
+  ~CallScope() {
+    g_launch_counter = nullptr;
+    if (prev_dev >= 0 && prev_dev != ctx->device) cudaSetDevice(prev_dev);
+  }
+};
+
+template <class F>
+pb_status guarded(pb_ctx* ctx, F&& f) {
+  if (!ctx) return PB_EINVAL;
+  try {
+    CallScope scope(ctx);
+    f();
+    ctx->last_error.clear();
+    return PB_OK;
+  } catch (const Error& e) {
+    ctx->last_error = e.msg;
+    if (e.status == PB_ECUDA) cudaGetLastError();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    ctx->last_error = "host allocation failed";
+    return PB_ENOMEM;
+  }
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+pb_opts resolve_opts(const pb_opts* o) {
+  pb_opts r;
+  pb_opts_default(&r);
+  if (o) r = *o;
+  PB_REQUIRE(r.count_type >= PB_SORT && r.count_type <= PB_SERIAL, PB_EINVAL, "count_type out of range");
+  PB_REQUIRE(r.rank_type >= PB_SIDE && r.rank_type <= PB_ADEG, PB_EINVAL, "rank_type out of range");
+  PB_REQUIRE(r.peel_type >= PB_PSORT && r.peel_type <= PB_PBATCHWA, PB_EINVAL, "peel_type out of range");
+  PB_REQUIRE(r.per_type >= PB_VERT && r.per_type <= PB_TOTAL, PB_EINVAL, "per_type out of range");
+  PB_REQUIRE(r.sched == PB_SCHED_PLAIN || r.sched == PB_SCHED_LEARNED, PB_EINVAL, "sched out of range");
+  return r;
+}
+
+__global__ void max_degree_kernel(const uint32_t* __restrict__ off, int64_t n, uint32_t* out) {
+  uint32_t m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, off[i + 1] - off[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void gather_vert_kernel(const int64_t* __restrict__ rc, const uint32_t* __restrict__ rank, int64_t base,
+                                   int64_t nc, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = rc[rank[base + i]];
+}
+
+// Device-side graph validation: offsets monotone, ids in range, lists strictly ascending.
+__global__ void validate_side_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ edg, int64_t n,
+                                     int64_t other_n, uint32_t* bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t b = off[i], e = off[i + 1];
+    if (e < b) { atomicOr(bad, 1u); continue; }
+    for (uint32_t k = b; k < e; ++k) {
+      uint32_t x = edg[k];
+      if ((int64_t)x >= other_n || (k > b && x <= edg[k - 1])) { atomicOr(bad, 2u); break; }
+    }
+  }
+}
+
+// PB_TRACE=1 in the environment: synchronise after every counting / peeling stage and print
+// its wall time to stderr (diagnostics; off by default).
+bool trace_on() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("PB_TRACE");
+    on = (e && *e && *e != '0') ? 1 : 0;
+  }
+  return on == 1;
+}
+
+struct Trace {
+  cudaStream_t s;
+  std::chrono::steady_clock::time_point t0;
+  explicit Trace(cudaStream_t st) : s(st), t0(std::chrono::steady_clock::now()) {}
+  void stage(const char* name) {
+    if (!trace_on()) return;
+    cudaError_t e = cudaStreamSynchronize(s);
+    auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[pb] %-10s %9.3f ms  %s\n", name, std::chrono::duration<double, std::milli>(t1 - t0).count(),
+            e == cudaSuccess ? "" : cudaGetErrorString(e));
+    fflush(stderr);
+    t0 = t1;
+  }
+};
+
+struct Timer {
+  cudaEvent_t ev[8];
+  int k = 0;
+  cudaStream_t s;
+  explicit Timer(cudaStream_t st) : s(st) {
+    for (auto& e : ev) PB_CUDA_TRY(cudaEventCreate(&e));
+  }
+  ~Timer() {
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  void mark() { PB_CUDA_TRY(cudaEventRecord(ev[k++], s)); }
+  double ms(int a, int b) {
+    float x = 0;
+    PB_CUDA_TRY(cudaEventElapsedTime(&x, ev[a], ev[b]));
+    return x;
+  }
+};
+
+int64_t out_len_of(const pb_graph* g, int per, int use_v) {
+  if (per == PB_VERT) return use_v ? g->nu : g->nv;
+  if (per == PB_EDGE) return g->m;
+  return 1;
+}
+
+// The whole counting pipeline; result (dense int64, length out_len_of) in out_dev.
+void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int use_v, int64_t* out_dev) {
+  cudaStream_t s = ctx->stream;
+  pb_stats& st = ctx->stats;
+  std::memset(&st, 0, sizeof(st));
+  int uv = 0;
+  int64_t wmin = 0, wv = 0, wu = 0;
+  cmp_wedge_counts(*g, &uv, &wmin, &wv, &wu, s);
+  if (use_v < 0) use_v = uv;
+  st.w_side = use_v ? wv : wu;
+  st.use_v = use_v;
+  Timer T(s);
+  Trace tr(s);
+  Ranked R;
+  T.mark();
+  vertex_order(*g, o.rank_type, use_v, R, s);
+  T.mark();
+  tr.stage("rank");
+  build_ranked_csr(*g, R, per == PB_EDGE, s);
+  T.mark();
+  tr.stage("relabel");
+  wedge_scan(R, s);
+  T.mark();
+  tr.stage("scan");
+  CountConfig cfg;
+  switch (o.count_type) {
+    case PB_BATCHS: case PB_BATCHWA: case PB_SERIAL: cfg.strategy = STRAT_DENSE; break;
+    case PB_SORT: case PB_ASORT: cfg.strategy = STRAT_SORT; break;
+    case PB_HIST: case PB_AHIST: cfg.strategy = STRAT_HIST; break;
+    default: cfg.strategy = STRAT_HASH; break;
+  }
+  DevBuf<uint32_t> chk;
+  if (check_mode()) {
+    chk.alloc(4, s);
+    PB_CUDA_TRY(cudaMemsetAsync(chk.get(), 0, 4 * sizeof(uint32_t), s));
+    validate_ranked(R, g->m, chk.get(), s);
+    cfg.err = chk.get();
+  }
+  DevBuf<int64_t> rc;
+  int64_t* target = out_dev;
+  if (per == PB_VERT) {
+    rc.alloc(R.n > 0 ? R.n : 1, s);
+    target = rc.get();
+  }
+  CountResult cr = count_ranked(R, per, target, cfg, s);
+  T.mark();
+  tr.stage("count");
+  if (chk.get()) {
+    uint32_t h[4];
+    PB_CUDA_TRY(cudaMemcpyAsync(h, chk.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    PB_REQUIRE(h[0] == 0, PB_ECUDA,
+               "checked mode: bounds violation code " + std::to_string(h[0]) + " index " +
+                   std::to_string(((uint64_t)h[2] << 32) | h[1]) + " aux " + std::to_string(h[3]));
+  }
+  if (per == PB_VERT) {
+    const int64_t nc = use_v ? g->nu : g->nv;
+    const int64_t base = use_v ? g->nv : 0;
+    if (nc > 0)
+      PB_LAUNCH(gather_vert_kernel, std::max(1, std::min(ceil_div(nc, 256), sm_count() * 8)), 256, 0, s, rc.get(),
+                R.rank.get(), base, nc, out_dev);
+  }
+  T.mark();
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  st.w_rank = R.w_rank;
+  st.n_big = cr.n_big;
+  st.ms_rank = T.ms(0, 1);
+  st.ms_relabel = T.ms(1, 2);
+  st.ms_scan = T.ms(2, 3);
+  st.ms_count = T.ms(3, 4);
+  st.ms_convert = T.ms(4, 5);
+  st.ms_agg_kernel = cr.agg_ms;
+}
+
+// Runs fn(out_dev) with a device buffer of len int64 and delivers it to a host or device
+// pointer.
+template <class F>
+void with_output(pb_ctx* ctx, int64_t* user_out, int64_t len, F&& fn) {
+  cudaStream_t s = ctx->stream;
+  if (len <= 0) { fn(nullptr); return; }
+  if (is_device_ptr(user_out)) {
+    fn(user_out);
+    return;
+  }
+  DevBuf<int64_t> tmp(len, s);
+  fn(tmp.get());
+  PB_CUDA_TRY(cudaMemcpyAsync(user_out, tmp.get(), sizeof(int64_t) * len, cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+void upload_graph(pb_ctx* ctx, const pb_csr* c, bool from_device, pb_graph** out) {
+  PB_REQUIRE(c && out, PB_EINVAL, "null argument");
+  PB_REQUIRE(c->nv >= 0 && c->nu >= 0 && c->m >= 0, PB_EINVAL, "negative size");
+  PB_REQUIRE(c->nv + c->nu < (int64_t)(1u << 31), PB_ETOOBIG, "nv + nu must stay below 2^31");
+  PB_REQUIRE(2 * c->m <= (int64_t)UINT32_MAX, PB_ETOOBIG, "2*m must fit 32-bit offsets");
+  cudaStream_t s = ctx->stream;
+  if (!from_device) {
+    char msg[256];
+    pb_status st = pb_csr_validate(c, msg, sizeof(msg));
+    PB_REQUIRE(st == PB_OK, st, std::string("invalid CSR: ") + msg);
+  }
+  auto* g = new pb_graph();
+  try {
+    g->device = ctx->device;
+    g->nv = c->nv; g->nu = c->nu; g->m = c->m;
+    g->offV.alloc(c->nv + 1, s);
+    g->offU.alloc(c->nu + 1, s);
+    g->edgV.alloc(c->m > 0 ? c->m : 1, s);
+    g->edgU.alloc(c->m > 0 ? c->m : 1, s);
+    const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PB_CUDA_TRY(cudaMemcpyAsync(g->offV.get(), c->offsetsV, sizeof(uint32_t) * (c->nv + 1), kind, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(g->offU.get(), c->offsetsU, sizeof(uint32_t) * (c->nu + 1), kind, s));
+    if (c->m > 0) {
+      PB_CUDA_TRY(cudaMemcpyAsync(g->edgV.get(), c->edgesV, sizeof(uint32_t) * c->m, kind, s));
+      PB_CUDA_TRY(cudaMemcpyAsync(g->edgU.get(), c->edgesU, sizeof(uint32_t) * c->m, kind, s));
+    }
+    DevBuf<uint32_t> mx(2, s);
+    PB_CUDA_TRY(cudaMemsetAsync(mx.get(), 0, 2 * sizeof(uint32_t), s));
+    const int grid = std::max(1, std::min(ceil_div(std::max(c->nv, c->nu) + 1, 256), sm_count() * 8));
+    if (c->nv) PB_LAUNCH(max_degree_kernel, grid, 256, 0, s, g->offV.get(), c->nv, mx.get());
+    if (c->nu) PB_LAUNCH(max_degree_kernel, grid, 256, 0, s, g->offU.get(), c->nu, mx.get());
+    if (from_device) {
+      uint32_t hoff[2];
+      PB_CUDA_TRY(cudaMemcpyAsync(&hoff[0], g->offV.get() + c->nv, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      PB_CUDA_TRY(cudaMemcpyAsync(&hoff[1], g->offU.get() + c->nu, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      PB_CUDA_TRY(cudaStreamSynchronize(s));
+      PB_REQUIRE(hoff[0] == (uint32_t)c->m && hoff[1] == (uint32_t)c->m, PB_EINVAL, "offsets[n] != m");
+      if (c->nv) PB_LAUNCH(validate_side_kernel, grid, 256, 0, s, g->offV.get(), g->edgV.get(), c->nv, c->nu, mx.get() + 1);
+      if (c->nu) PB_LAUNCH(validate_side_kernel, grid, 256, 0, s, g->offU.get(), g->edgU.get(), c->nu, c->nv, mx.get() + 1);
+    }
+    uint32_t h[2];
+    PB_CUDA_TRY(cudaMemcpyAsync(h, mx.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    PB_REQUIRE(h[1] == 0, PB_EINVAL, "invalid CSR (unsorted list or id out of range)");
+    g->max_deg = h[0];
+    PB_REQUIRE(g->max_deg < (1u << 23), PB_ETOOBIG, "maximum degree must stay below 2^23");
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  *out = g;
+}
+
+}  // namespace
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" {
+
+int pb_abi_version(void) { return PB_ABI_VERSION; }
+
+void pb_opts_default(pb_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->count_type = PB_SERIAL;
+  o->rank_type = PB_ADEG;
+  o->peel_type = PB_PBATCHS;
+  o->per_type = PB_VERT;
+  o->max_wedges = 2577500000LL;
+  o->max_array_size = 23090996160LL;
+  o->sched = PB_SCHED_PLAIN;
+  o->autotune = 0;
+  o->use_v = -1;
+}
+
+pb_status pb_ctx_create(int device, void* stream, pb_ctx** out) {
+  if (!out) return PB_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PB_ECUDA;
+  }
+  if (device < 0 || device >= ndev) return PB_EINVAL;
+  auto* c = new (std::nothrow) pb_ctx();
+  if (!c) return PB_ENOMEM;
+  c->device = device;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) { delete c; return PB_ECUDA; }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      cudaSetDevice(prev);
+      return PB_ECUDA;
+    }
+    c->own_stream = true;
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  cudaGetLastError();
+  cudaSetDevice(prev);
+  *out = c;
+  return PB_OK;
+}
+
+pb_status pb_ctx_destroy(pb_ctx* ctx) {
+  if (!ctx) return PB_EINVAL;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  cudaSetDevice(prev);
+  delete ctx;
+  return PB_OK;
+}
+
+const char* pb_last_error(const pb_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+pb_status pb_get_stats(const pb_ctx* ctx, pb_stats* out) {
+  if (!ctx || !out) return PB_EINVAL;
+  *out = ctx->stats;
+  return PB_OK;
+}
+
+int64_t pb_kernel_launches(const pb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+pb_status pb_graph_upload(pb_ctx* ctx, const pb_csr* host, pb_graph** out) {
+  return guarded(ctx, [&] { upload_graph(ctx, host, false, out); });
+}
+
+pb_status pb_graph_from_device(pb_ctx* ctx, const pb_csr* dev, pb_graph** out) {
+  return guarded(ctx, [&] { upload_graph(ctx, dev, true, out); });
+}
+
+pb_status pb_graph_destroy(pb_graph* g) {
+  if (!g) return PB_EINVAL;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(g->device);
+  cudaDeviceSynchronize();
+  delete g;
+  cudaSetDevice(prev);
+  return PB_OK;
+}
+
+pb_status pb_graph_dims(const pb_graph* g, int64_t* nv, int64_t* nu, int64_t* m) {
+  if (!g) return PB_EINVAL;
+  if (nv) *nv = g->nv;
+  if (nu) *nu = g->nu;
+  if (m) *m = g->m;
+  return PB_OK;
+}
+
+pb_status pb_cmp_wedge_counts(pb_ctx* ctx, const pb_graph* g, int32_t* use_v, int64_t* num_wedges) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(g && use_v && num_wedges, PB_EINVAL, "null argument");
+    int uv = 0;
+    int64_t w = 0, wv = 0, wu = 0;
+    cmp_wedge_counts(*g, &uv, &w, &wv, &wu, ctx->stream);
+    *use_v = uv;
+    *num_wedges = w;
+  });
+}
+
+pb_status pb_edge_to_idxs(pb_ctx* ctx, const pb_graph* g, int32_t use_v, uint32_t* eti) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(g && eti, PB_EINVAL, "null argument");
+    if (g->m == 0) return;
+    if (is_device_ptr(eti)) {
+      edge_to_idxs(*g, use_v != 0, eti, ctx->stream);
+      PB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    } else {
+      DevBuf<uint32_t> tmp(g->m, ctx->stream);
+      edge_to_idxs(*g, use_v != 0, tmp.get(), ctx->stream);
+      PB_CUDA_TRY(cudaMemcpyAsync(eti, tmp.get(), sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, ctx->stream));
+      PB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+  });
+}
+
+static pb_status count_entry(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out, int per) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(g && out, PB_EINVAL, "null argument");
+    pb_opts o = resolve_opts(opts);
+    int use_v = o.use_v;
+    if (use_v >= 0) use_v = use_v != 0;
+    if (use_v < 0) {
+      int uv = 0;
+      int64_t w = 0, wv = 0, wu = 0;
+      cmp_wedge_counts(*g, &uv, &w, &wv, &wu, ctx->stream);
+      use_v = uv;
+    }
+    const int64_t len = out_len_of(g, per, use_v);
+    if (per == PB_TOTAL && len > 0 && !is_device_ptr(out)) {
+      DevBuf<int64_t> tmp(1, ctx->stream);
+      run_count(ctx, g, o, per, use_v, tmp.get());
+      PB_CUDA_TRY(cudaMemcpyAsync(out, tmp.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+      PB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      return;
+    }
+    with_output(ctx, out, len, [&](int64_t* dev) {
+      if (dev) run_count(ctx, g, o, per, use_v, dev);
+    });
+  });
+}
+
+pb_status pb_count_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out) {
+  return count_entry(ctx, g, opts, out, PB_VERT);
+}
+pb_status pb_count_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out) {
+  return count_entry(ctx, g, opts, out, PB_EDGE);
+}
+pb_status pb_count_total(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, int64_t* out) {
+  return count_entry(ctx, g, opts, out, PB_TOTAL);
+}
+
+static pb_status peel_entry(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* counts, int64_t* res,
+                            bool edges) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(g && counts && res, PB_EINVAL, "null argument");
+    pb_opts o = resolve_opts(opts);
+    int use_v = o.use_v;
+    if (use_v >= 0) use_v = use_v != 0;
+    if (use_v < 0) {
+      int uv = 0;
+      int64_t w = 0, wv = 0, wu = 0;
+      cmp_wedge_counts(*g, &uv, &w, &wv, &wu, ctx->stream);
+      use_v = uv;
+    }
+    cudaStream_t s = ctx->stream;
+    const int64_t len = edges ? g->m : (use_v ? g->nu : g->nv);
+    if (len <= 0) return;
+    DevBuf<int64_t> cin;
+    const int64_t* cdev = counts;
+    if (!is_device_ptr(counts)) {
+      cin.alloc(len, s);
+      PB_CUDA_TRY(cudaMemcpyAsync(cin.get(), counts, sizeof(int64_t) * len, cudaMemcpyHostToDevice, s));
+      cdev = cin.get();
+    }
+    Timer T(s);
+    with_output(ctx, res, len, [&](int64_t* dev) {
+      T.mark();
+      PeelResult pr = edges ? peel_edges(*g, use_v, cdev, dev, s) : peel_vertices(*g, use_v, cdev, dev, s);
+      T.mark();
+      PB_CUDA_TRY(cudaStreamSynchronize(s));
+      ctx->stats.ms_peel = T.ms(0, 1);
+      ctx->stats.peel_rounds = pr.rounds;
+      ctx->stats.peel_work = pr.work;
+    });
+  });
+}
+
+pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* counts, int64_t* tip) {
+  return peel_entry(ctx, g, opts, counts, tip, false);
+}
+pb_status pb_peel_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* ecounts, int64_t* wing) {
+  return peel_entry(ctx, g, opts, ecounts, wing, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,522 @@
+// Wedge aggregation and butterfly accumulation on the ranked CSR.
+//
+// Semantics (CountWorkEfficientParallel, butterfly_count.h:1218-1320; the per-edge and total
+// variants butterfly_ecount.h:1334-1429 and butterfly_count_total.h:662-749): for every
+// endpoint i, the wedges are (i, v, u2) with v in N(i), u2 in N(v), u2 < min(i, v); w(u2) is
+// the number of wedges of i that end in u2.  Then
+//   VERT : tagged endpoints i and u2 gain C(w,2); tagged centres v gain w-1 per wedge;
+//   EDGE : edges (i,v) and (v,u2) gain w-1 per wedge;
+//   TOTAL: the sum of C(w,2).
+// Endpoint and centre are on opposite sides, so for one endpoint either the centre credits or
+// the endpoint credits matter, never both.
+//
+// Aggregators (the multiplicity table w):
+//   warp  : endpoints with W_i <= small_w; one warp, an open-addressing table in shared memory
+//           (keys u2, values w), linear probing, insert by atomicCAS / atomicAdd.
+//   block : larger endpoints, one CTA per endpoint taken from a global work counter; the table
+//           is a dense shared-memory window over [0, i) (BATCHS-style dense counters), a
+//           shared-memory hash table, or a per-CTA dense array in global scratch memory when
+//           neither fits.
+// The wedge list of an endpoint is flattened: each chunk of neighbours gets an inclusive scan
+// of its prefix lengths, and lane/thread t locates its neighbour by a branchless binary search
+// over that scan, so consecutive threads read consecutive entries of N(v) (coalesced).
+#include <algorithm>
+
+#include "pb_engine.cuh"
+#include "pb_prims.cuh"
+
+namespace pb {
+
+namespace {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kWarpTable = 1024;  // slots per warp (keys + values = 8 KiB)
+constexpr int kWarpsPerBlockSmall = 8;
+
+enum Per { VERT = 0, EDGE = 1, TOTAL = 2 };
+
+struct Params {
+  const uint32_t* __restrict__ off;
+  const uint32_t* __restrict__ adj;
+  const uint32_t* __restrict__ pref;
+  const uint32_t* __restrict__ eout;
+  const int64_t* __restrict__ wsum;
+  int64_t n;
+  int per;
+  int64_t* out;
+  int64_t out_len;  // entries of out
+  int64_t m2;       // slots of the ranked CSR
+  uint32_t* err;    // record of the first bounds violation {code, index lo, index hi, aux}
+};
+
+// Records the first bounds violation (checked mode only).
+__device__ __noinline__ void record_violation(uint32_t* err, uint32_t code, uint64_t idx, uint32_t aux) {
+  if (atomicCAS(&err[0], 0u, code) == 0u) {
+    err[1] = (uint32_t)idx;
+    err[2] = (uint32_t)(idx >> 32);
+    err[3] = aux;
+  }
+}
+
+// out[idx] += v.  Indices derived from memory are bounds-checked; a violation is recorded
+// (and reported as an error by the host) instead of being accessed.
+__device__ __forceinline__ void credit(const Params& P, uint64_t idx, int64_t v, uint32_t code) {
+  if (idx >= (uint64_t)P.out_len) { record_violation(P.err, code, idx, 0); return; }
+  atomic_add_i64(&P.out[idx], v);
+}
+
+__device__ __forceinline__ bool slot_ok(const Params& P, uint64_t slot, uint32_t code) {
+  if (slot >= (uint64_t)P.m2) { record_violation(P.err, code, slot, 0); return false; }
+  return true;
+}
+
+// Fibonacci hashing: the high bits of key * 2^32/phi, folded into the table size.
+__device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t mask) {
+  return __umulhi(key * 0x9E3779B1u, mask + 1u) & mask;
+}
+
+// Insert-or-increment.  Tables are sized to at least twice the wedge count, so a probe
+// sequence never exceeds the table size; the bound turns a broken invariant into a recorded
+// error instead of an endless loop.
+__device__ __forceinline__ bool table_insert(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    uint32_t k = keys[h];
+    if (k == key) { atomicAdd(&vals[h], 1u); return true; }
+    if (k == kEmpty) {
+      uint32_t prev = atomicCAS(&keys[h], kEmpty, key);
+      if (prev == kEmpty || prev == key) { atomicAdd(&vals[h], 1u); return true; }
+    }
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t table_find(const uint32_t* keys, const uint32_t* vals, uint32_t mask,
+                                               uint32_t key) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    uint32_t k = keys[h];
+    if (k == key) return vals[h];
+    if (k == kEmpty) return 0;  // unreachable for keys that were inserted
+    h = (h + 1) & mask;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ uint32_t next_pow2(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
+
+// Iterates every wedge of endpoint i (slots [b, e) of the ranked CSR) with one warp.
+// f(j, vt, slot2, u2t): j = slot of (i, v), vt = tagged v, slot2 = slot of (v, u2), u2t = tagged u2.
+template <class F>
+__device__ __forceinline__ void warp_wedges(uint32_t b, uint32_t e, const Params& P, F&& f) {
+  const unsigned lane = lane_id();
+  for (uint32_t j0 = b; j0 < e; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    uint32_t L = 0, vt = 0, vs = 0;
+    if (j < e) {
+      L = P.pref[j];
+      vt = P.adj[j];
+      if ((vt >> 1) < P.n) vs = P.off[vt >> 1];
+      else { record_violation(P.err, 28, vt, j); L = 0; }
+    }
+    const uint32_t incl = warp_inclusive_scan(L);
+    const uint32_t excl = incl - L;
+    const uint32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t t0 = 0; t0 < T; t0 += 32) {
+      const uint32_t t = t0 + lane;
+      uint32_t lo = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        uint32_t x = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+        if (x <= t) lo += step;
+      }
+      const uint32_t ex = __shfl_sync(0xffffffffu, excl, lo);
+      const uint32_t vsj = __shfl_sync(0xffffffffu, vs, lo);
+      const uint32_t vtj = __shfl_sync(0xffffffffu, vt, lo);
+      if (t < T) {
+        const uint32_t slot2 = vsj + (t - ex);
+        if (slot_ok(P, slot2, 20)) f(j0 + lo, vtj, slot2, P.adj[slot2]);
+      }
+    }
+  }
+}
+
+// Per-thread accumulator of per-(i,v) credits, flushed when the neighbour slot changes.
+struct SlotAcc {
+  uint32_t j = kEmpty;
+  int64_t acc = 0;
+  __device__ __forceinline__ void flush(const Params& P) {
+    if (j != kEmpty && acc) {
+      if (!slot_ok(P, j, 10)) return;
+      if (P.per == VERT) credit(P, P.adj[j] >> 1, acc, 11);
+      else credit(P, P.eout[j], acc, 12);
+    }
+    acc = 0;
+  }
+  __device__ __forceinline__ void add(const Params& P, uint32_t jj, int64_t x) {
+    if (jj != j) { flush(P); j = jj; }
+    acc += x;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) count_warp_kernel(Params P, int small_w) {
+  extern __shared__ uint32_t smem_w[];
+  const unsigned lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  uint32_t* keys = smem_w + wib * (2 * kWarpTable);
+  uint32_t* vals = keys + kWarpTable;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int64_t total = 0;
+  for (int64_t i = warp; i < P.n; i += nwarps) {
+    const int64_t W = P.wsum[i + 1] - P.wsum[i];
+    if (W <= 0 || W > small_w) {
+      if (W < 0 && lane == 0) record_violation(P.err, 34, (uint64_t)i, 0);
+      continue;
+    }
+    const uint32_t b = P.off[i], e = P.off[i + 1];
+    const bool tag_i = !(P.adj[b] & 1u);
+    const bool need_center = P.per == EDGE || (P.per == VERT && !tag_i);
+    const uint32_t tsize = max(64u, next_pow2(2u * (uint32_t)W));
+    const uint32_t mask = tsize - 1;
+    for (uint32_t s = lane; s < tsize; s += 32) { keys[s] = kEmpty; vals[s] = 0; }
+    __syncwarp();
+    warp_wedges(b, e, P, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+      if (!table_insert(keys, vals, mask, u2t >> 1)) record_violation(P.err, 25, u2t >> 1, (uint32_t)i);
+    });
+    __syncwarp();
+    if (need_center) {
+      SlotAcc acc;
+      warp_wedges(b, e, P, [&](uint32_t jj, uint32_t, uint32_t slot2, uint32_t u2t) {
+        const uint32_t w = table_find(keys, vals, mask, u2t >> 1);
+        if (w > 1) {
+          if (P.per == EDGE) credit(P, P.eout[slot2], (int64_t)(w - 1), 13);
+          acc.add(P, jj, (int64_t)(w - 1));
+        }
+      });
+      acc.flush(P);
+    } else {
+      int64_t mine = 0;
+      for (uint32_t s = lane; s < tsize; s += 32) {
+        const uint32_t k = keys[s];
+        if (k == kEmpty) continue;
+        const int64_t w = vals[s];
+        if (w < 2) continue;
+        const int64_t bf = w * (w - 1) / 2;
+        mine += bf;
+        if (P.per == VERT) credit(P, k, bf, 14);
+      }
+      if (P.per == VERT) {
+        mine = warp_sum(mine);
+        if (lane == 0 && mine) credit(P, i, mine, 15);
+      } else {
+        total += mine;
+      }
+    }
+    __syncwarp();
+  }
+  if (P.per == TOTAL) {
+    total = warp_sum(total);
+    if (lane == 0 && total) atomic_add_i64(P.out, total);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+constexpr int kBlock = 512;
+
+struct BlockShared {
+  uint32_t incl[kBlock];
+  uint32_t vs[kBlock];
+  uint32_t vt[kBlock];
+  uint32_t scan[32];
+  int64_t red[32];
+  uint32_t item;
+};
+
+__device__ __forceinline__ uint32_t block_inclusive_scan_u32(uint32_t x, uint32_t* smem, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint32_t incl = warp_inclusive_scan(x);
+  if (lane == 31) smem[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t v = lane < nwarps ? smem[lane] : 0u;
+    v = warp_inclusive_scan(v);
+    smem[lane] = v;
+  }
+  __syncthreads();
+  incl += warp > 0 ? smem[warp - 1] : 0u;
+  total = smem[nwarps - 1];
+  return incl;
+}
+
+__device__ __forceinline__ int64_t block_sum_i64(int64_t x, int64_t* smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  x = warp_sum(x);
+  __syncthreads();
+  if (lane == 0) smem[warp] = x;
+  __syncthreads();
+  int64_t t = 0;
+  if (warp == 0) {
+    t = lane < nwarps ? smem[lane] : 0;
+    t = warp_sum(t);
+  }
+  return t;  // valid in thread 0
+}
+
+// Iterates every wedge of endpoint i with the whole CTA.
+template <class F>
+__device__ __forceinline__ void block_wedges(uint32_t b, uint32_t e, const Params& P, BlockShared& S, F&& f) {
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t j0 = b; j0 < e; j0 += kBlock) {
+    const uint32_t j = j0 + tid;
+    uint32_t L = 0, vt = 0, vs = 0;
+    if (j < e) {
+      L = P.pref[j];
+      vt = P.adj[j];
+      if ((vt >> 1) < P.n) vs = P.off[vt >> 1];
+      else { record_violation(P.err, 29, vt, j); L = 0; }
+    }
+    uint32_t T;
+    const uint32_t incl = block_inclusive_scan_u32(L, S.scan, T);
+    S.incl[tid] = incl;
+    S.vs[tid] = vs;
+    S.vt[tid] = vt;
+    __syncthreads();
+    for (uint32_t t0 = 0; t0 < T; t0 += kBlock) {
+      const uint32_t t = t0 + tid;
+      if (t < T) {
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+          if (S.incl[lo + step - 1] <= t) lo += step;
+        const uint32_t ex = lo ? S.incl[lo - 1] : 0u;
+        const uint32_t slot2 = S.vs[lo] + (t - ex);
+        if (slot_ok(P, slot2, 21)) f(j0 + lo, S.vt[lo], slot2, P.adj[slot2]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+enum Mode : uint32_t { MODE_DENSE = 0, MODE_HASH = 1, MODE_GLOBAL = 2 };
+
+__global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uint32_t* __restrict__ items,
+                                                             const uint32_t* __restrict__ n_items_dev,
+                                                             uint32_t* cursor, uint32_t* gscratch,
+                                                             uint32_t cap_dense, uint32_t cap_hash) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BlockShared& S = *reinterpret_cast<BlockShared*>(smem_raw);
+  uint32_t* table = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(BlockShared) + 15) & ~size_t(15)));
+  uint32_t* gcnt = gscratch ? gscratch + (size_t)blockIdx.x * (size_t)P.n : nullptr;
+  const uint32_t n_items = *n_items_dev;
+  int64_t total = 0;
+  while (true) {
+    if (threadIdx.x == 0) S.item = atomicAdd(cursor, 1u);
+    __syncthreads();
+    const uint32_t q = S.item;
+    __syncthreads();
+    if (q >= n_items) break;
+    const uint32_t i = items[q];
+    const int64_t W = P.wsum[i + 1] - P.wsum[i];
+    const uint32_t b = P.off[i], e = P.off[i + 1];
+    const bool tag_i = !(P.adj[b] & 1u);
+    const bool need_center = P.per == EDGE || (P.per == VERT && !tag_i);
+    Mode mode;
+    if (i <= cap_dense && (uint64_t)i <= 4ull * (uint64_t)W) mode = MODE_DENSE;
+    else if ((uint64_t)2 * W <= cap_hash) mode = MODE_HASH;
+    else if (i <= cap_dense) mode = MODE_DENSE;
+    else mode = MODE_GLOBAL;
+    uint32_t tsize = 0, mask = 0;
+    uint32_t* keys = table;
+    uint32_t* vals = table + cap_hash;
+    if (mode == MODE_DENSE) {
+      for (uint32_t s = threadIdx.x; s < i; s += kBlock) table[s] = 0;
+    } else if (mode == MODE_HASH) {
+      tsize = max(64u, next_pow2(2u * (uint32_t)W));
+      mask = tsize - 1;
+      for (uint32_t s = threadIdx.x; s < tsize; s += kBlock) { keys[s] = kEmpty; vals[s] = 0; }
+    }
+    __syncthreads();
+    // Phase 1: multiplicities.
+    if (mode == MODE_DENSE) {
+      block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+        if ((u2t >> 1) >= i) { record_violation(P.err, 22, u2t >> 1, i); return; }
+        atomicAdd(&table[u2t >> 1], 1u);
+      });
+    } else if (mode == MODE_HASH) {
+      block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+        if (!table_insert(keys, vals, mask, u2t >> 1)) record_violation(P.err, 26, u2t >> 1, i);
+      });
+    } else {
+      block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+        if ((u2t >> 1) >= P.n) { record_violation(P.err, 23, u2t >> 1, i); return; }
+        atomicAdd(&gcnt[u2t >> 1], 1u);
+      });
+    }
+    __syncthreads();
+    if (need_center) {
+      // Phase 2: centre / edge credits.
+      SlotAcc acc;
+      block_wedges(b, e, P, S, [&](uint32_t jj, uint32_t, uint32_t slot2, uint32_t u2t) {
+        const uint32_t u2 = u2t >> 1;
+        uint32_t w;
+        if (u2 >= (mode == MODE_DENSE ? i : (uint32_t)P.n)) { record_violation(P.err, 24, u2, i); return; }
+        if (mode == MODE_DENSE) w = table[u2];
+        else if (mode == MODE_HASH) w = table_find(keys, vals, mask, u2);
+        else w = gcnt[u2];
+        if (w > 1) {
+          if (P.per == EDGE) credit(P, P.eout[slot2], (int64_t)(w - 1), 13);
+          acc.add(P, jj, (int64_t)(w - 1));
+        }
+      });
+      acc.flush(P);
+      __syncthreads();
+      if (mode == MODE_GLOBAL) {  // restore the zero invariant of the scratch array
+        block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+          if ((u2t >> 1) < P.n) gcnt[u2t >> 1] = 0;
+        });
+        __syncthreads();
+      }
+    } else {
+      // Phase 3: endpoint credits, once per distinct u2.
+      int64_t mine = 0;
+      if (mode == MODE_DENSE) {
+        for (uint32_t s = threadIdx.x; s < i; s += kBlock) {
+          const int64_t w = table[s];
+          if (w >= 2) {
+            const int64_t bf = w * (w - 1) / 2;
+            mine += bf;
+            if (P.per == VERT) credit(P, s, bf, 16);
+          }
+        }
+      } else if (mode == MODE_HASH) {
+        for (uint32_t s = threadIdx.x; s < tsize; s += kBlock) {
+          const uint32_t k = keys[s];
+          if (k == kEmpty) continue;
+          const int64_t w = vals[s];
+          if (w >= 2) {
+            const int64_t bf = w * (w - 1) / 2;
+            mine += bf;
+            if (P.per == VERT) credit(P, k, bf, 17);
+          }
+        }
+      } else {
+        block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+          if ((u2t >> 1) >= P.n) { record_violation(P.err, 27, u2t >> 1, i); return; }
+          const int64_t w = atomicExch(&gcnt[u2t >> 1], 0u);
+          if (w >= 2) {
+            const int64_t bf = w * (w - 1) / 2;
+            mine += bf;
+            if (P.per == VERT) credit(P, u2t >> 1, bf, 18);
+          }
+        });
+      }
+      if (P.per == VERT) {
+        const int64_t s = block_sum_i64(mine, S.red);
+        if (threadIdx.x == 0 && s) credit(P, i, s, 19);
+      } else {
+        total += mine;
+      }
+      __syncthreads();
+    }
+  }
+  if (P.per == TOTAL) {
+    const int64_t s = block_sum_i64(total, S.red);
+    if (threadIdx.x == 0 && s) atomic_add_i64(P.out, s);
+  }
+}
+
+__global__ void classify_endpoints_kernel(const int64_t* __restrict__ wsum, int64_t n, int small_w, uint32_t cap_dense,
+                                          uint32_t cap_hash, uint32_t* items, uint32_t* counts /* [0]=big [1]=global */) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t W = wsum[i + 1] - wsum[i];
+    if (W <= small_w) continue;
+    items[atomicAdd(&counts[0], 1u)] = (uint32_t)i;
+    const bool dense_ok = (uint64_t)i <= cap_dense;
+    const bool hash_ok = (uint64_t)2 * W <= cap_hash;
+    if (!dense_ok && !hash_ok) atomicAdd(&counts[1], 1u);
+  }
+}
+
+}  // namespace
+
+CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConfig& cfg, cudaStream_t s) {
+  CountResult res;
+  const int64_t n = R.n;
+  const int64_t out_len = per == VERT ? n : (per == EDGE ? R.m2 / 2 : 1);
+  if (out_len > 0) PB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int64_t) * out_len, s));
+  if (n == 0 || R.w_rank == 0) return res;
+  Params P{R.off.get(), R.adj.get(), R.pref.get(), per == EDGE ? R.eout.get() : nullptr, R.wsum.get(), n, per, out,
+           out_len, R.m2, nullptr};
+  DevBuf<uint32_t> err_local;
+  if (cfg.err) {
+    P.err = cfg.err;
+  } else {
+    err_local.alloc(4, s);
+    PB_CUDA_TRY(cudaMemsetAsync(err_local.get(), 0, 4 * sizeof(uint32_t), s));
+    P.err = err_local.get();
+  }
+  const int sms = sm_count();
+  const int small_w = std::min(cfg.small_w, kWarpTable / 2);
+
+  // Block aggregator geometry.
+  const size_t shared_fixed = (sizeof(BlockShared) + 15) & ~size_t(15);
+  const size_t table_bytes = (size_t)cfg.smem_bytes > shared_fixed ? (size_t)cfg.smem_bytes - shared_fixed : 0;
+  const uint32_t cap_dense = (uint32_t)(table_bytes / 4);
+  uint32_t cap_hash = 1;
+  while ((size_t)cap_hash * 2 * 8 <= table_bytes) cap_hash <<= 1;  // slots; keys + values
+  if (cap_hash < 64) cap_hash = 64;
+
+  DevBuf<uint32_t> items(n, s), counts(3, s);
+  PB_CUDA_TRY(cudaMemsetAsync(counts.get(), 0, 3 * sizeof(uint32_t), s));
+  PB_LAUNCH(classify_endpoints_kernel, std::max(1, std::min(ceil_div(n, 256), sms * 8)), 256, 0, s, R.wsum.get(), n,
+            small_w, cap_dense, cap_hash, items.get(), counts.get());
+  uint32_t hc[2];
+  PB_CUDA_TRY(cudaMemcpyAsync(hc, counts.get(), sizeof(hc), cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  res.n_big = (int)hc[0];
+
+  cudaEvent_t e0, e1;
+  PB_CUDA_TRY(cudaEventCreate(&e0));
+  PB_CUDA_TRY(cudaEventCreate(&e1));
+  PB_CUDA_TRY(cudaEventRecord(e0, s));
+  {
+    const int smem = kWarpsPerBlockSmall * 2 * kWarpTable * (int)sizeof(uint32_t);
+    static bool attr_set = false;
+    if (!attr_set) {
+      PB_CUDA_TRY(cudaFuncSetAttribute(count_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      attr_set = true;
+    }
+    PB_LAUNCH(count_warp_kernel, sms * 3, kWarpsPerBlockSmall * 32, smem, s, P, small_w);
+  }
+  DevBuf<uint32_t> gscratch;
+  if (hc[0] > 0) {
+    const int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * cfg.blocks_per_sm);
+    if (hc[1] > 0) {
+      gscratch.alloc((size_t)grid * (size_t)n, s);
+      PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
+    }
+    PB_CUDA_TRY(cudaFuncSetAttribute(count_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cfg.smem_bytes));
+    PB_LAUNCH(count_block_kernel, grid, kBlock, cfg.smem_bytes, s, P, items.get(), counts.get(), counts.get() + 2,
+              gscratch.get(), cap_dense, cap_hash);
+  }
+  PB_CUDA_TRY(cudaEventRecord(e1, s));
+  PB_CUDA_TRY(cudaEventSynchronize(e1));
+  {
+    uint32_t h[4];
+    PB_CUDA_TRY(cudaMemcpy(h, P.err, sizeof(h), cudaMemcpyDeviceToHost));
+    PB_REQUIRE(h[0] == 0, PB_ECUDA,
+               "aggregation: bounds violation code " + std::to_string(h[0]) + " index " +
+                   std::to_string(((uint64_t)h[2] << 32) | h[1]) + " aux " + std::to_string(h[3]));
+  }
+  float ms = 0;
+  PB_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  res.agg_ms = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return res;
+}
+
+}  // namespace pb

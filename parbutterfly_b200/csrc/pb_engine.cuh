@@ -1,0 +1,80 @@
+// Internal structures shared by the ranking, counting and peeling stages.
+#pragma once
+
+#include <vector>
+
+#include "pb_common.cuh"
+
+struct pb_graph {
+  int device = 0;
+  int64_t nv = 0, nu = 0, m = 0;
+  // Device copy of the two-sided CSR (never modified after upload).
+  pb::DevBuf<uint32_t> offV, edgV, offU, edgU;
+  uint32_t max_deg = 0;
+};
+
+namespace pb {
+
+// Timing of one counting call (milliseconds, CUDA events on the context stream).
+struct StageTimes {
+  double rank = 0, relabel = 0, scan = 0, count = 0, convert = 0, agg_kernel = 0;
+};
+
+// Ranked single CSR of n = nv + nu vertices (rankGraph / rankGraphEdges,
+// butterfly_utils.h:579-700): row r holds (rank << 1 | on_count_side) of the neighbours of the
+// vertex of rank r, ascending.
+struct Ranked {
+  int64_t n = 0, m2 = 0;
+  int use_v = 1;
+  DevBuf<uint32_t> order;  // order[r] = combined id (V ids 0..nv-1, then nv + U id)
+  DevBuf<uint32_t> rank;   // rank[combined id]
+  DevBuf<uint32_t> off;    // n+1
+  DevBuf<uint32_t> adj;    // 2m tagged ranks
+  DevBuf<uint32_t> eout;   // 2m output edge index (per-edge counting only)
+  DevBuf<uint32_t> pref;   // 2m: wedges of slot (i,j) = #{u2 in N(v): u2 < min(i,v)}
+  DevBuf<int64_t> wsum;    // n+1: exclusive prefix of per-endpoint wedge counts
+  int64_t w_rank = 0;
+  uint32_t max_deg = 0;
+};
+
+// Ranking stage (pb_rank.cu).
+void degrees_combined(const pb_graph& g, uint32_t* deg, cudaStream_t s);
+void cmp_wedge_counts(const pb_graph& g, int* use_v, int64_t* w_min, int64_t* wv, int64_t* wu, cudaStream_t s);
+void vertex_order(const pb_graph& g, int rank_type, int use_v, Ranked& R, cudaStream_t s);
+void build_ranked_csr(const pb_graph& g, Ranked& R, bool with_eout, cudaStream_t s);
+void wedge_scan(Ranked& R, cudaStream_t s);
+void edge_to_idxs(const pb_graph& g, int use_v, uint32_t* eti, cudaStream_t s);
+
+// Counting stage (pb_count.cu).  per: 0 VERT (out: rank-space counts [n]), 1 EDGE (out: [m]
+// in output edge order), 2 TOTAL (out: [1]).  `strategy` selects the aggregator.
+enum Strategy { STRAT_HASH = 0, STRAT_DENSE = 1, STRAT_SORT = 2, STRAT_HIST = 3, STRAT_AUTO = 4 };
+struct CountConfig {
+  int strategy = STRAT_AUTO;
+  int small_w = 512;          // endpoints with W_i <= small_w go to the warp aggregator
+  int block_threads = 512;    // threads of the block aggregator
+  int smem_bytes = 192 * 1024;  // dynamic shared memory of the block aggregator
+  int blocks_per_sm = 1;
+  int split_w = 0;            // endpoints above this many wedges are split across CTAs (0: auto)
+  uint32_t* err = nullptr;    // checked mode: device record of the first bounds violation
+};
+
+// Checked mode (PB_CHECK=1): kernels bounds-check indices read from memory and record the
+// first violation instead of accessing out of bounds; the ranked CSR is validated after the
+// relabel.  Off by default.
+bool check_mode();
+void validate_ranked(const Ranked& R, int64_t m, uint32_t* err, cudaStream_t s);
+struct CountResult {
+  int n_big = 0;
+  double agg_ms = 0;
+};
+CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConfig& cfg, cudaStream_t s);
+
+// Peeling stage (pb_peel.cu).
+struct PeelResult {
+  int64_t rounds = 0;
+  int64_t work = 0;
+};
+PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s);
+PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s);
+
+}  // namespace pb

@@ -1,0 +1,849 @@
+// Tip (vertex) and wing (edge) peeling on the device.
+//
+// Semantics (Peel / PeelOrigParallel, butterfly_peel.h:647-711,896-934; PeelE /
+// PeelEOrigParallel, butterfly_epeel.h:339-443,519-569; updateBuckets,
+// butterfly_putils.h:1027-1115): items start in bucket D = their butterfly count.  Each round
+// takes every unpeeled item whose bucket equals the current minimum k (the frontier):
+//   tip : for each frontier vertex u and each two-hop neighbour u2 != u, the C(w(u,u2), 2)
+//         shared butterflies leave u2's count;
+//   wing: each butterfly that contains a frontier edge and no edge peeled in an earlier round
+//         is removed once, by its frontier edge of smallest index, and its other edges lose 1.
+// Every touched unpeeled item moves to bucket max(count, k).  Buckets are 64-bit (the
+// reference's are 32-bit, ligra/bucket.h:15-16, exact only below 2^32 - 1).
+//
+// Device design: one cooperative persistent kernel runs all rounds.  Phases are separated by
+// a grid barrier whose wait is bounded in time (on expiry the kernel records PB_ETIMEOUT and
+// returns; the context stays usable).  Buckets are kept as a near/far split: the near list
+// holds the unpeeled items whose bucket lies below a window bound; each round scans only the
+// near list (frontier extraction fused with the next minimum), and the window advances (one
+// pass over the alive list, a log2 histogram of distances to the minimum) when the near list
+// runs dry.  Frontier items with little work run one per warp; heavy ones one per CTA.
+#include <algorithm>
+#include <cstring>
+
+#include "pb_engine.cuh"
+#include "pb_prims.cuh"
+
+namespace pb {
+
+namespace {
+
+constexpr int kPT = 512;
+constexpr int kPW = kPT / 32;
+constexpr int kWarpSlots = 1024;   // per-warp table slots (keys + values: 8 KiB)
+constexpr int kBlockSlots = 16384; // per-CTA table slots (128 KiB), shares memory with warp tables
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr unsigned long long kInf = ~0ull;
+constexpr uint8_t ALIVE = 0, ACTIVE = 1, PEELED = 2;
+constexpr unsigned ERR_TIMEOUT = 1u;
+constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;  // 60 s per wait
+
+struct Ctl {
+  unsigned long long nm[2];       // next minimum per round parity
+  unsigned long long k_lo, win_hi;
+  unsigned long long rounds, work;
+  unsigned flen_small[2], flen_big[2];
+  unsigned tlen[2];
+  unsigned cur_small[2], cur_big[2];
+  unsigned near_len;
+  unsigned alive;                 // unpeeled items
+  unsigned alen[2];               // alive list lengths
+  unsigned hist[66];
+  unsigned bar_count, bar_gen, err;
+};
+
+struct Lists {
+  const uint32_t* offK;  // count side: vertex -> centre ids
+  const uint32_t* edgK;
+  const uint32_t* offC;  // centre side: vertex -> count-side ids (positions = output edge index)
+  const uint32_t* edgC;
+  const uint32_t* eti;   // count-side list position -> output edge index (wing only)
+  const uint32_t* center_of;  // output edge index -> centre vertex (wing only)
+  const int64_t* S;      // per count-side vertex then per centre vertex: sum of neighbour degrees (wing)
+  const int64_t* wk;     // per count-side vertex: two-hop wedges sum(deg(v) - 1) (tip)
+  int64_t nK, nC;
+};
+
+struct Work {
+  int64_t* D;        // buckets (final: tip / wing numbers)
+  int64_t* cnt;      // butterfly counts
+  uint8_t* state;
+  uint8_t* in_near;
+  uint32_t* touched;
+  uint32_t* alist[2];
+  uint32_t* near;
+  uint32_t* fsmall[2];
+  uint32_t* fbig[2];
+  uint32_t* tlist[2];
+  uint32_t* gscratch;  // per-CTA dense scratch (dense counters / probe markers)
+  int64_t gscratch_len;
+  int64_t N;           // items
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid barrier for a cooperative launch (all CTAs co-resident).  Bounded: a wait longer than
+// kBarrierTimeoutNs sets ERR_TIMEOUT and returns false.
+__device__ bool grid_barrier(Ctl* ctl) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &ctl->bar_gen;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
+    ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&ctl->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1u);
+    } else {
+      const unsigned long long t0 = globaltimer_ns();
+      while (*vgen == gen) {
+        if (*(volatile unsigned*)&ctl->err) { ok = 0; break; }
+        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+          atomicOr(&ctl->err, ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*(volatile unsigned*)&ctl->err) ok = 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Fibonacci hashing: the high bits of key * 2^32/phi, folded into the table size.
+__device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t mask) {
+  return __umulhi(key * 0x9E3779B1u, mask + 1u) & mask;
+}
+
+// Tables are sized to at least twice their key count, so probe sequences stay shorter than
+// the table; the bounds turn a broken invariant into a recorded error, not an endless loop.
+constexpr unsigned ERR_TABLE = 2u;
+
+__device__ __forceinline__ void t_add(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key, Ctl* ctl) {
+  uint32_t h = hslot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    uint32_t k = keys[h];
+    if (k == key) { atomicAdd(&vals[h], 1u); return; }
+    if (k == kEmpty) {
+      uint32_t prev = atomicCAS(&keys[h], kEmpty, key);
+      if (prev == kEmpty || prev == key) { atomicAdd(&vals[h], 1u); return; }
+    }
+    h = (h + 1) & mask;
+  }
+  atomicOr(&ctl->err, ERR_TABLE);
+}
+
+// Unique-key insert of (key, val).
+__device__ __forceinline__ void t_put(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key, uint32_t val,
+                                      Ctl* ctl) {
+  uint32_t h = hslot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    uint32_t prev = atomicCAS(&keys[h], kEmpty, key);
+    if (prev == kEmpty) { vals[h] = val; return; }
+    h = (h + 1) & mask;
+  }
+  atomicOr(&ctl->err, ERR_TABLE);
+}
+
+__device__ __forceinline__ bool t_get(const uint32_t* keys, const uint32_t* vals, uint32_t mask, uint32_t key,
+                                      uint32_t& val) {
+  uint32_t h = hslot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    uint32_t k = keys[h];
+    if (k == key) { val = vals[h]; return true; }
+    if (k == kEmpty) return false;
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t np2(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
+
+struct Shared {
+  uint32_t incl[kPT];
+  uint32_t sb[kPT];
+  uint32_t scan[32];
+  unsigned long long red[32];
+  uint32_t item;
+  unsigned hist[66];
+};
+
+// Flattened two-level iteration by one warp: first(j, L, sb) gives the second-level range
+// [sb, sb + L) of first-level position j in [b, e); f(j, q) is called once per pair.
+template <class First, class F>
+__device__ __forceinline__ void warp_iter(uint32_t b, uint32_t e, First&& first, F&& f) {
+  const unsigned lane = lane_id();
+  for (uint32_t j0 = b; j0 < e; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    uint32_t L = 0, sb = 0;
+    if (j < e) first(j, L, sb);
+    const uint32_t incl = warp_inclusive_scan(L);
+    const uint32_t excl = incl - L;
+    const uint32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t t0 = 0; t0 < T; t0 += 32) {
+      const uint32_t t = t0 + lane;
+      uint32_t lo = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        uint32_t x = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+        if (x <= t) lo += step;
+      }
+      const uint32_t ex = __shfl_sync(0xffffffffu, excl, lo);
+      const uint32_t s = __shfl_sync(0xffffffffu, sb, lo);
+      if (t < T) f(j0 + lo, s + (t - ex));
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* smem, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint32_t incl = warp_inclusive_scan(x);
+  if (lane == 31) smem[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t v = lane < nwarps ? smem[lane] : 0u;
+    v = warp_inclusive_scan(v);
+    smem[lane] = v;
+  }
+  __syncthreads();
+  incl += warp > 0 ? smem[warp - 1] : 0u;
+  total = smem[nwarps - 1];
+  __syncthreads();
+  return incl;
+}
+
+// Same iteration by the whole CTA.
+template <class First, class F>
+__device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f) {
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t j0 = b; j0 < e; j0 += kPT) {
+    const uint32_t j = j0 + tid;
+    uint32_t L = 0, sb = 0;
+    if (j < e) first(j, L, sb);
+    uint32_t T;
+    const uint32_t incl = block_incl_scan(L, S.scan, T);
+    S.incl[tid] = incl;
+    S.sb[tid] = sb;
+    __syncthreads();
+    for (uint32_t t0 = 0; t0 < T; t0 += kPT) {
+      const uint32_t t = t0 + tid;
+      if (t < T) {
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t step = kPT / 2; step > 0; step >>= 1)
+          if (S.incl[lo + step - 1] <= t) lo += step;
+        const uint32_t ex = lo ? S.incl[lo - 1] : 0u;
+        f(j0 + lo, S.sb[lo] + (t - ex));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void touch(const Work& W, Ctl* ctl, unsigned par, uint32_t x) {
+  if (W.touched[x] == 0 && atomicExch(&W.touched[x], 1u) == 0u) W.tlist[par][atomicAdd(&ctl->tlen[par], 1u)] = x;
+}
+
+__device__ __forceinline__ void dec(const Work& W, Ctl* ctl, unsigned par, uint32_t x, int64_t amount) {
+  if (W.state[x] == ALIVE) {
+    atomic_add_i64(&W.cnt[x], -amount);
+    touch(W, ctl, par, x);
+  }
+}
+
+// Per-thread accumulator keyed by the first-level position.
+struct PosAcc {
+  uint32_t j = kEmpty;
+  int64_t acc = 0;
+};
+
+// ---- tip: process one frontier vertex -------------------------------------------------------
+__device__ void tip_item_warp(const Lists& G, const Work& W, Ctl* ctl, unsigned par, uint32_t u, uint32_t* keys,
+                              uint32_t* vals, unsigned long long& work) {
+  const unsigned lane = lane_id();
+  const int64_t wk = G.wk[u];
+  const uint32_t tsize = max(64u, np2(2u * (uint32_t)wk));
+  const uint32_t mask = tsize - 1;
+  for (uint32_t s = lane; s < tsize; s += 32) { keys[s] = kEmpty; vals[s] = 0; }
+  __syncwarp();
+  warp_iter(G.offK[u], G.offK[u + 1],
+            [&](uint32_t j, uint32_t& L, uint32_t& sb) {
+              const uint32_t v = G.edgK[j];
+              sb = G.offC[v];
+              L = G.offC[v + 1] - sb;
+            },
+            [&](uint32_t, uint32_t q) {
+              const uint32_t u2 = G.edgC[q];
+              if (u2 != u) t_add(keys, vals, mask, u2, ctl);
+            });
+  __syncwarp();
+  for (uint32_t s = lane; s < tsize; s += 32) {
+    const uint32_t k = keys[s];
+    if (k == kEmpty) continue;
+    const int64_t w = vals[s];
+    if (w >= 2) dec(W, ctl, par, k, w * (w - 1) / 2);
+  }
+  if (lane == 0) work += (unsigned long long)wk;
+  __syncwarp();
+}
+
+__device__ void tip_item_block(const Lists& G, const Work& W, Ctl* ctl, unsigned par, uint32_t u, uint32_t* table,
+                               Shared& S, unsigned long long& work) {
+  const int64_t wk = G.wk[u];
+  const bool hash = (uint64_t)2 * (uint64_t)wk <= (uint64_t)kBlockSlots;
+  uint32_t* keys = table;
+  uint32_t* vals = table + kBlockSlots;
+  uint32_t* gcnt = W.gscratch + (size_t)blockIdx.x * (size_t)W.gscratch_len;
+  const uint32_t tsize = hash ? max(64u, np2(2u * (uint32_t)wk)) : 0u;
+  const uint32_t mask = tsize - 1;
+  if (hash)
+    for (uint32_t s = threadIdx.x; s < tsize; s += kPT) { keys[s] = kEmpty; vals[s] = 0; }
+  __syncthreads();
+  auto first = [&](uint32_t j, uint32_t& L, uint32_t& sb) {
+    const uint32_t v = G.edgK[j];
+    sb = G.offC[v];
+    L = G.offC[v + 1] - sb;
+  };
+  block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+    const uint32_t u2 = G.edgC[q];
+    if (u2 == u) return;
+    if (hash) t_add(keys, vals, mask, u2, ctl);
+    else atomicAdd(&gcnt[u2], 1u);
+  });
+  __syncthreads();
+  if (hash) {
+    for (uint32_t s = threadIdx.x; s < tsize; s += kPT) {
+      const uint32_t k = keys[s];
+      if (k == kEmpty) continue;
+      const int64_t w = vals[s];
+      if (w >= 2) dec(W, ctl, par, k, w * (w - 1) / 2);
+    }
+  } else {
+    block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+      const uint32_t u2 = G.edgC[q];
+      if (u2 == u) return;
+      const int64_t w = atomicExch(&gcnt[u2], 0u);
+      if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
+    });
+  }
+  if (threadIdx.x == 0) work += (unsigned long long)wk;
+  __syncthreads();
+}
+
+// ---- wing: process one frontier edge --------------------------------------------------------
+// Orientation A (walk from the centre v): probe set N(u) (centre -> edge), first level N(v)
+// (u2, edge e2), second level N(u2) (v2, edge e3), probe v2 -> e4.
+// Orientation B (walk from u): probe set N(v) (count-side vertex -> edge), first level N(u)
+// (v2, e4), second level N(v2) (u2, e3), probe u2 -> e2.  Both find the same butterflies.
+struct WingEdge {
+  uint32_t e1, u, v;
+  bool from_v;
+};
+
+__device__ __forceinline__ bool skip_edge(const Work& W, uint32_t e, uint32_t e1) {
+  const uint8_t s = W.state[e];
+  return s == PEELED || (s == ACTIVE && e < e1);
+}
+
+template <bool kBlockLevel>
+__device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par, const WingEdge& E, uint32_t* keys,
+                          uint32_t* vals, uint32_t slots, Shared* S, unsigned long long& work) {
+  const uint32_t rank = kBlockLevel ? threadIdx.x : lane_id();
+  const uint32_t gsize = kBlockLevel ? kPT : 32;
+  auto sync = [&]() {
+    if (kBlockLevel) __syncthreads();
+    else __syncwarp();
+  };
+  // probe set
+  uint32_t pb, pe;
+  if (E.from_v) { pb = G.offK[E.u]; pe = G.offK[E.u + 1]; }
+  else { pb = G.offC[E.v]; pe = G.offC[E.v + 1]; }
+  const uint32_t psize = pe - pb;
+  const bool hash = 2 * psize <= slots;
+  uint32_t* mark = W.gscratch + (size_t)blockIdx.x * (size_t)W.gscratch_len;
+  const uint32_t tsize = hash ? max(64u, np2(2u * psize)) : 0u;
+  const uint32_t mask = tsize - 1;
+  if (hash)
+    for (uint32_t s = rank; s < tsize; s += gsize) keys[s] = kEmpty;
+  sync();
+  for (uint32_t p = pb + rank; p < pe; p += gsize) {
+    uint32_t key, e;
+    if (E.from_v) { key = G.edgK[p]; e = G.eti[p]; }
+    else { key = G.edgC[p]; e = p; }
+    if (W.state[e] == PEELED) continue;
+    if (hash) t_put(keys, vals, mask, key, e, ctl);
+    else mark[key] = e + 1;
+  }
+  sync();
+  auto probe = [&](uint32_t key, uint32_t& e) -> bool {
+    if (hash) return t_get(keys, vals, mask, key, e);
+    const uint32_t x = mark[key];
+    if (!x) return false;
+    e = x - 1;
+    return true;
+  };
+  PosAcc acc;
+  unsigned long long my_work = 0;
+  auto flush = [&]() {
+    if (acc.j != kEmpty && acc.acc) dec(W, ctl, par, E.from_v ? acc.j : G.eti[acc.j], acc.acc);
+    acc.acc = 0;
+  };
+  if (E.from_v) {
+    auto first = [&](uint32_t p, uint32_t& L, uint32_t& sb) {
+      const uint32_t u2 = G.edgC[p];
+      if (u2 == E.u || skip_edge(W, p, E.e1)) { L = 0; sb = 0; return; }
+      sb = G.offK[u2];
+      L = G.offK[u2 + 1] - sb;
+    };
+    auto f = [&](uint32_t p, uint32_t q) {
+      ++my_work;
+      const uint32_t v2 = G.edgK[q];
+      if (v2 == E.v) return;
+      const uint32_t e3 = G.eti[q];
+      if (skip_edge(W, e3, E.e1)) return;
+      uint32_t e4;
+      if (!probe(v2, e4) || (W.state[e4] == ACTIVE && e4 < E.e1)) return;
+      dec(W, ctl, par, e3, 1);
+      dec(W, ctl, par, e4, 1);
+      if (p != acc.j) { flush(); acc.j = p; }
+      acc.acc += 1;
+    };
+    if (kBlockLevel) block_iter(G.offC[E.v], G.offC[E.v + 1], *S, first, f);
+    else warp_iter(G.offC[E.v], G.offC[E.v + 1], first, f);
+  } else {
+    auto first = [&](uint32_t q, uint32_t& L, uint32_t& sb) {
+      const uint32_t v2 = G.edgK[q];
+      if (v2 == E.v || skip_edge(W, G.eti[q], E.e1)) { L = 0; sb = 0; return; }
+      sb = G.offC[v2];
+      L = G.offC[v2 + 1] - sb;
+    };
+    auto f = [&](uint32_t q, uint32_t p3) {
+      ++my_work;
+      const uint32_t u2 = G.edgC[p3];
+      if (u2 == E.u) return;
+      if (skip_edge(W, p3, E.e1)) return;
+      uint32_t e2;
+      if (!probe(u2, e2) || (W.state[e2] == ACTIVE && e2 < E.e1)) return;
+      dec(W, ctl, par, e2, 1);
+      dec(W, ctl, par, p3, 1);
+      if (q != acc.j) { flush(); acc.j = q; }
+      acc.acc += 1;
+    };
+    if (kBlockLevel) block_iter(G.offK[E.u], G.offK[E.u + 1], *S, first, f);
+    else warp_iter(G.offK[E.u], G.offK[E.u + 1], first, f);
+  }
+  flush();
+  work += my_work;
+  sync();
+  if (!hash) {  // clear the dense markers
+    for (uint32_t p = pb + rank; p < pe; p += gsize) mark[E.from_v ? G.edgK[p] : G.edgC[p]] = 0;
+  }
+  sync();
+}
+
+// ---- the persistent kernel ------------------------------------------------------------------
+// Wing items run on one warp when their work is small and their probe set fits a warp table.
+struct Classify {
+  int64_t small_work;
+  __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const { return G.wk[u] <= 512; }
+  __device__ __forceinline__ bool wing_from_v(const Lists& G, uint32_t v, uint32_t u) const {
+    return G.S[G.nK + v] <= G.S[u];
+  }
+  __device__ __forceinline__ bool wing_small(const Lists& G, uint32_t e) const {
+    const uint32_t v = G.center_of[e], u = G.edgC[e];
+    const bool fv = wing_from_v(G, v, u);
+    const int64_t work = fv ? G.S[G.nK + v] : G.S[u];
+    const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
+    return work <= small_work && 2 * psize <= (uint32_t)kWarpSlots;
+  }
+};
+
+template <bool kWing>
+__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Classify cls) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Shared& S = *reinterpret_cast<Shared*>(smem_raw);
+  uint32_t* pool = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(Shared) + 15) & ~size_t(15)));
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* wkeys = pool + warp * (2 * kWarpSlots);
+  uint32_t* wvals = wkeys + kWarpSlots;
+  const unsigned gtid = blockIdx.x * kPT + threadIdx.x;
+  const unsigned gthreads = gridDim.x * kPT;
+  unsigned alist_cur = 0;
+  unsigned long long work = 0;
+  for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = (uint32_t)x;
+  if (!grid_barrier(ctl)) return;
+
+  for (unsigned long long r = 0;; ++r) {
+    const unsigned par = (unsigned)(r & 1ull), npar = par ^ 1u;
+    if (*(volatile unsigned*)&ctl->alive == 0) break;
+    unsigned long long k = *(volatile unsigned long long*)&ctl->nm[par];
+    if (k == kInf) {
+      // ---- window advance (no unpeeled item left in the near list): compact the alive list
+      // and take its minimum; a log2 histogram of distances to the minimum picks the window
+      // bound; the near list is rebuilt from the alive list.
+      const unsigned na = alist_cur ^ 1u;
+      const unsigned alen = *(volatile unsigned*)&ctl->alen[alist_cur];
+      unsigned long long mn = kInf;
+      for (unsigned q = gtid; q < alen; q += gthreads) {
+        const uint32_t x = W.alist[alist_cur][q];
+        if (W.state[x] != ALIVE) continue;
+        W.alist[na][atomicAdd(&ctl->alen[na], 1u)] = x;
+        mn = min(mn, (unsigned long long)W.D[x]);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      if (lane == 0 && mn != kInf) atomicMin(&ctl->k_lo, mn);
+      if (threadIdx.x < 66) S.hist[threadIdx.x] = 0;
+      if (blockIdx.x == 0) {
+        // The previous advance's histogram was last read before two barriers ago.
+        if (threadIdx.x < 66) ctl->hist[threadIdx.x] = 0;
+        if (threadIdx.x == 0) ctl->near_len = 0;
+      }
+      if (!grid_barrier(ctl)) return;
+      const unsigned long long klo = *(volatile unsigned long long*)&ctl->k_lo;
+      const unsigned alen2 = *(volatile unsigned*)&ctl->alen[na];
+      for (unsigned q = gtid; q < alen2; q += gthreads) {
+        const unsigned long long d = (unsigned long long)W.D[W.alist[na][q]] - klo;
+        atomicAdd(&S.hist[d ? 64 - __clzll(d) : 0], 1u);
+      }
+      __syncthreads();
+      if (threadIdx.x < 66 && S.hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], S.hist[threadIdx.x]);
+      if (!grid_barrier(ctl)) return;
+      // Every CTA derives the same bound: the smallest B with >= target items at distance < 2^B.
+      const unsigned target = max(32768u, alen2 / 64u);
+      unsigned cum = 0;
+      int B = 0;
+      for (; B < 65; ++B) {
+        cum += *(volatile unsigned*)&ctl->hist[B];
+        if (cum >= target) break;
+      }
+      unsigned long long hi = kInf;
+      if (B < 63) {
+        const unsigned long long span = 1ull << B;
+        if (klo <= kInf - span) hi = klo + span;
+      }
+      for (unsigned q = gtid; q < alen2; q += gthreads) {
+        const uint32_t x = W.alist[na][q];
+        if (hi == kInf || (unsigned long long)W.D[x] < hi) {
+          W.in_near[x] = 1;
+          W.near[atomicAdd(&ctl->near_len, 1u)] = x;
+        }
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->win_hi = hi;
+        ctl->alen[alist_cur] = 0;  // read by every CTA before the first barrier
+        ctl->k_lo = kInf;          // read by every CTA right after the first barrier
+      }
+      alist_cur = na;
+      if (!grid_barrier(ctl)) return;
+      k = klo;
+    }
+    const unsigned long long win_hi = *(volatile unsigned long long*)&ctl->win_hi;
+    // ---- phase F: the frontier is every near item in bucket k; the minimum of the other near
+    // items is the first part of the next round's minimum.
+    {
+      const unsigned nl = *(volatile unsigned*)&ctl->near_len;
+      unsigned long long mn = kInf;
+      for (unsigned q = gtid; q < nl; q += gthreads) {
+        const uint32_t x = W.near[q];
+        if (W.state[x] != ALIVE) continue;
+        const unsigned long long d = (unsigned long long)W.D[x];
+        if (d == k) {
+          W.state[x] = ACTIVE;
+          const bool small = kWing ? cls.wing_small(G, x) : cls.tip_small(G, x);
+          if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
+          else W.fbig[par][atomicAdd(&ctl->flen_big[par], 1u)] = x;
+        } else {
+          mn = min(mn, d);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      if (lane == 0 && mn != kInf) atomicMin(&ctl->nm[npar], mn);
+      if (blockIdx.x == 0 && threadIdx.x == 0) {  // slots of the previous round, no longer read
+        ctl->flen_small[npar] = 0;
+        ctl->flen_big[npar] = 0;
+        ctl->tlen[npar] = 0;
+        ctl->cur_small[npar] = 0;
+        ctl->cur_big[npar] = 0;
+      }
+    }
+    if (!grid_barrier(ctl)) return;
+    // ---- phase P: process the frontier (small items per warp, then heavy items per CTA).
+    {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->nm[par] = kInf;  // every CTA has read it
+      const unsigned ns = *(volatile unsigned*)&ctl->flen_small[par];
+      while (true) {
+        unsigned q = 0;
+        if (lane == 0) q = atomicAdd(&ctl->cur_small[par], 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= ns) break;
+        const uint32_t x = W.fsmall[par][q];
+        if (kWing) {
+          WingEdge E;
+          E.e1 = x;
+          E.v = G.center_of[x];
+          E.u = G.edgC[x];
+          E.from_v = cls.wing_from_v(G, E.v, E.u);
+          wing_item<false>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work);
+        } else {
+          tip_item_warp(G, W, ctl, par, x, wkeys, wvals, work);
+        }
+      }
+      __syncthreads();  // warp tables and the CTA table share memory
+      const unsigned nb = *(volatile unsigned*)&ctl->flen_big[par];
+      while (true) {
+        if (threadIdx.x == 0) S.item = atomicAdd(&ctl->cur_big[par], 1u);
+        __syncthreads();
+        const unsigned q = S.item;
+        __syncthreads();
+        if (q >= nb) break;
+        const uint32_t x = W.fbig[par][q];
+        if (kWing) {
+          WingEdge E;
+          E.e1 = x;
+          E.v = G.center_of[x];
+          E.u = G.edgC[x];
+          E.from_v = cls.wing_from_v(G, E.v, E.u);
+          wing_item<true>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work);
+        } else {
+          tip_item_block(G, W, ctl, par, x, pool, S, work);
+        }
+      }
+    }
+    if (!grid_barrier(ctl)) return;
+    // ---- phase U: touched items move to bucket max(count, k) (all unpeeled items are above
+    // k here); those entering the window join the near list and feed the next minimum.
+    {
+      const unsigned nt = *(volatile unsigned*)&ctl->tlen[par];
+      unsigned long long mn = kInf;
+      for (unsigned q = gtid; q < nt; q += gthreads) {
+        const uint32_t x = W.tlist[par][q];
+        W.touched[x] = 0;
+        if (W.state[x] != ALIVE) continue;
+        const int64_t c = W.cnt[x];
+        const int64_t nd = c > (int64_t)k ? c : (int64_t)k;
+        W.D[x] = nd;
+        if ((unsigned long long)nd < win_hi) {
+          mn = min(mn, (unsigned long long)nd);
+          if (!W.in_near[x]) {
+            W.in_near[x] = 1;
+            W.near[atomicAdd(&ctl->near_len, 1u)] = x;
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      if (lane == 0 && mn != kInf) atomicMin(&ctl->nm[npar], mn);
+      const unsigned ns = *(volatile unsigned*)&ctl->flen_small[par];
+      const unsigned nb = *(volatile unsigned*)&ctl->flen_big[par];
+      for (unsigned q = gtid; q < ns + nb; q += gthreads) {
+        const uint32_t x = q < ns ? W.fsmall[par][q] : W.fbig[par][q - ns];
+        W.state[x] = PEELED;
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->alive -= ns + nb;
+        ctl->rounds += 1;
+      }
+    }
+    if (!grid_barrier(ctl)) return;
+  }
+  unsigned long long w = work;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+  if (lane == 0 && w) atomicAdd(&ctl->work, w);
+}
+
+// ---- set-up kernels -------------------------------------------------------------------------
+__global__ void peel_init_kernel(const int64_t* __restrict__ counts, int64_t N, int64_t* D, int64_t* cnt,
+                                 uint8_t* state, uint8_t* in_near, uint32_t* touched) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < N; x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = counts[x];
+    D[x] = c;
+    cnt[x] = c;
+    state[x] = ALIVE;
+    in_near[x] = 0;
+    touched[x] = 0;
+  }
+}
+
+// wk[u] = sum over v in N(u) of (deg(v) - 1): the two-hop wedges of a count-side vertex.
+__global__ void tip_work_kernel(const uint32_t* __restrict__ offK, const uint32_t* __restrict__ edgK,
+                                const uint32_t* __restrict__ offC, int64_t nK, int64_t* wk) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t u = warp; u < nK; u += nwarps) {
+    int64_t s = 0;
+    for (uint32_t j = offK[u] + lane; j < offK[u + 1]; j += 32) {
+      const uint32_t v = edgK[j];
+      s += (int64_t)(offC[v + 1] - offC[v]) - 1;
+    }
+    s = warp_sum(s);
+    if (lane == 0) wk[u] = s;
+  }
+}
+
+// S[x] = sum over neighbours y of deg(y), for both sides (count side first).
+__global__ void nbr_degree_sum_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ edg,
+                                      const uint32_t* __restrict__ off_other, int64_t n, int64_t* S) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t x = warp; x < n; x += nwarps) {
+    int64_t s = 0;
+    for (uint32_t j = off[x] + lane; j < off[x + 1]; j += 32) {
+      const uint32_t y = edg[j];
+      s += (int64_t)(off_other[y + 1] - off_other[y]);
+    }
+    s = warp_sum(s);
+    if (lane == 0) S[x] = s;
+  }
+}
+
+__global__ void center_of_kernel(const uint32_t* __restrict__ offC, int64_t nC, uint32_t* center_of) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t v = warp; v < nC; v += nwarps)
+    for (uint32_t j = offC[v] + lane; j < offC[v + 1]; j += 32) center_of[j] = (uint32_t)v;
+}
+
+__global__ void max_i64_kernel(const int64_t* __restrict__ a, int64_t n, unsigned long long* out) {
+  unsigned long long m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, (unsigned long long)a[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+int grid_for(int64_t n, int per_block = 256) { return std::max(1, std::min(ceil_div(n, per_block), sm_count() * 16)); }
+
+template <bool kWing>
+PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t* out, cudaStream_t s) {
+  PeelResult res;
+  Lists G{};
+  G.offK = use_v ? g.offU.get() : g.offV.get();
+  G.edgK = use_v ? g.edgU.get() : g.edgV.get();
+  G.offC = use_v ? g.offV.get() : g.offU.get();
+  G.edgC = use_v ? g.edgV.get() : g.edgU.get();
+  G.nK = use_v ? g.nu : g.nv;
+  G.nC = use_v ? g.nv : g.nu;
+  const int64_t N = kWing ? g.m : G.nK;
+  if (N == 0) return res;
+  PB_REQUIRE(N < (int64_t)UINT32_MAX, PB_ETOOBIG, "too many items to peel");
+
+  DevBuf<int64_t> cnt(N, s), wk, Sx;
+  DevBuf<uint32_t> eti, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
+  DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), tl0(N, s), tl1(N, s);
+  DevBuf<uint8_t> state(N, s), in_near(N, s);
+  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, out, cnt.get(), state.get(), in_near.get(),
+            touched.get());
+  bool need_scratch = false;
+  int64_t scratch_len = 0;
+  if (kWing) {
+    eti.alloc(g.m, s);
+    center_of.alloc(g.m, s);
+    Sx.alloc(G.nK + G.nC, s);
+    edge_to_idxs(g, use_v, eti.get(), s);
+    PB_LAUNCH(center_of_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.nC, center_of.get());
+    if (G.nK) PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, Sx.get());
+    if (G.nC)
+      PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.edgC, G.offK, G.nC, Sx.get() + G.nK);
+    G.eti = eti.get();
+    G.center_of = center_of.get();
+    G.S = Sx.get();
+    need_scratch = 2ull * g.max_deg > (uint64_t)kBlockSlots;
+    scratch_len = std::max(G.nK, G.nC);
+  } else {
+    wk.alloc(G.nK, s);
+    PB_LAUNCH(tip_work_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, wk.get());
+    G.wk = wk.get();
+    DevBuf<unsigned long long> mx(1, s);
+    PB_CUDA_TRY(cudaMemsetAsync(mx.get(), 0, sizeof(unsigned long long), s));
+    PB_LAUNCH(max_i64_kernel, grid_for(G.nK), 256, 0, s, wk.get(), G.nK, mx.get());
+    unsigned long long hmx = 0;
+    PB_CUDA_TRY(cudaMemcpyAsync(&hmx, mx.get(), sizeof(hmx), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    need_scratch = 2ull * hmx > (uint64_t)kBlockSlots;
+    scratch_len = G.nK;
+  }
+
+  const size_t smem = ((sizeof(Shared) + 15) & ~size_t(15)) + (size_t)kBlockSlots * 2 * sizeof(uint32_t);
+  auto kern = peel_kernel<kWing>;
+  PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  PB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
+  PB_REQUIRE(per_sm >= 1, PB_ECUDA, "peeling kernel does not fit on an SM");
+  const int grid = sm_count() * per_sm;
+
+  DevBuf<uint32_t> gscratch;
+  if (need_scratch) {
+    gscratch.alloc((size_t)grid * (size_t)scratch_len, s);
+    PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
+  }
+  Work W{};
+  W.D = out;
+  W.cnt = cnt.get();
+  W.state = state.get();
+  W.in_near = in_near.get();
+  W.touched = touched.get();
+  W.alist[0] = alist0.get();
+  W.alist[1] = alist1.get();
+  W.near = nearl.get();
+  W.fsmall[0] = fs0.get();
+  W.fsmall[1] = fs1.get();
+  W.fbig[0] = fb0.get();
+  W.fbig[1] = fb1.get();
+  W.tlist[0] = tl0.get();
+  W.tlist[1] = tl1.get();
+  W.gscratch = gscratch.get();
+  W.gscratch_len = scratch_len;
+  W.N = N;
+
+  Ctl hctl;
+  std::memset(&hctl, 0, sizeof(hctl));
+  hctl.nm[0] = kInf;
+  hctl.nm[1] = kInf;
+  hctl.k_lo = kInf;
+  hctl.alive = (unsigned)N;
+  hctl.alen[0] = (unsigned)N;
+  DevBuf<Ctl> ctl(1, s);
+  PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  Classify cls{8192};
+  Ctl* ctl_ptr = ctl.get();
+  void* args[] = {&G, &W, &ctl_ptr, &cls};
+  PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
+  if (g_launch_counter) ++*g_launch_counter;
+  PB_CUDA_TRY(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  PB_REQUIRE(!(hctl.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
+  PB_REQUIRE(hctl.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
+  PB_REQUIRE(hctl.alive == 0, PB_ECUDA, "peeling ended with unpeeled items");
+  res.rounds = (int64_t)hctl.rounds;
+  res.work = (int64_t)hctl.work;
+  return res;
+}
+
+}  // namespace
+
+PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s) {
+  return run_peel<false>(g, use_v, counts_dev, tip_dev, s);
+}
+
+PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s) {
+  return run_peel<true>(g, use_v, ecounts_dev, wing_dev, s);
+}
+
+}  // namespace pb
