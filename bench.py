@@ -1,0 +1,338 @@
+"""Benchmark of the wedge-aggregation hot path on the bipartite R-MAT workload.
+
+Workload (default): bipartite R-MAT, |V| = 2^20, |U| = 2^18, (a,b,c,d) = (.55,.15,.15,.15),
+m = 2^24 distinct edges, seed 2 (seeded synthetic stand-in; no public dataset is named).
+One step = ACOCORE ranking + per-edge counting with HASH aggregation (-rankType ACOCORE
+-per EDGE -countType HASH) + wing peeling (PBATCHS semantics) of the resulting counts.
+
+metric "wedges/s": W_rank (the wedges the ranked traversal enumerates, countWedgesScan) per
+second of a whole step (count + peel).  `value` runs on a device-resident graph with device
+outputs; `e2e` is the same step through the C ABI with pinned host buffers (graph upload,
+count download, count upload for peeling, wing download inside the timed region).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): every rank runs an independent replica (the path does not shard on one
+node; there is no data-path collective) and rank 0 reports the aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "workload": "bipartite R-MAT 2^20 x 2^18, m=2^24, (a,b,c,d)=(.55,.15,.15,.15), seed 2; "
+                "ACOCORE rank, per-EDGE HASH count + wing peel",
+    "nv": 1 << 20, "nu": 1 << 18, "m": 1 << 24, "rank_type": "ACOCORE", "per": "EDGE", "count_type": "HASH",
+    "peel_type": "BATCHS", "l2": "inputs larger than L2 plus a 256 MiB L2 flush before every timed step",
+}
+# Bounded CPU sample: the same generator and flags at 1/32 of the edges.
+CPU_SAMPLE = {"log_nv": 15, "log_nu": 13, "m": 1 << 19}
+REF_STEP_SAMPLE = {"log_nv": 14, "log_nu": 12, "m": 1 << 18}
+
+
+def make_graph(log_nv=20, log_nu=18, m=1 << 24):
+    from parbutterfly_b200.graph import BipartiteGraph
+    return BipartiteGraph.rmat(log_nv, log_nu, m, 0.55, 0.15, 0.15, 0.15, 2)
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_cpu_baseline(sample, threads, steps=1):
+    """The reference's own CPU implementation (oracle/_ref, OpenMP build) on a bounded sample."""
+    import oracle
+    g = make_graph(sample["log_nv"], sample["log_nu"], sample["m"])
+    wr = oracle.ranked_wedges(g, "ACOCORE")
+    times = []
+    for _ in range(steps):
+        r = oracle.run_reference(g, "EDGE", "HASH", "ACOCORE", "BATCHS", threads=threads, timeout=1200)
+        times.append(r["count_s"] + r["peel_s"])
+    return g, wr, times, r
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    threads = os.cpu_count() or 1
+    if not oracle.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness_omp not built (reference tree absent at build time)"}))
+        return
+    s = REF_STEP_SAMPLE
+    g = make_graph(s["log_nv"], s["log_nu"], s["m"])
+    wr = oracle.ranked_wedges(g, "ACOCORE")
+    for _ in range(args.warmup):
+        oracle.run_reference(g, "EDGE", "HASH", "ACOCORE", "BATCHS", threads=threads, timeout=1200)
+    times = []
+    for _ in range(args.steps):
+        r = oracle.run_reference(g, "EDGE", "HASH", "ACOCORE", "BATCHS", threads=threads, timeout=1200)
+        times.append(r["count_s"] + r["peel_s"])
+    step = sum(times) / len(times)
+    value = wr / step
+    sample = (f"bipartite R-MAT 2^{s['log_nv']} x 2^{s['log_nu']}, m=2^{s['m'].bit_length() - 1}, same (a,b,c,d) "
+              f"and flags; W_rank={wr}; count {r['count_s']:.2f} s + wing peel {r['peel_s']:.2f} s per step")
+    line = {
+        "impl": "reference", "metric": "wedges/s", "value": value, "unit": "wedges/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": dict(WORKLOAD, sample=sample),
+        "cpu_baseline": {"value": value, "unit": "wedges/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "wedges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def our_arm(args, rank, world, local):
+    import numpy as np
+    import torch
+    from parbutterfly_b200 import butterflies as pb
+
+    g = make_graph()
+    # A dedicated (non-default) stream shared by torch and the library, so CUDA events recorded
+    # by torch bracket the library's kernels.
+    stream = torch.cuda.Stream(local)
+    torch.cuda.set_stream(stream)
+    ctx = pb.Context(local, stream=stream.cuda_stream)
+    dg = ctx.upload(g)
+    use_v, w_side = pb.cmp_wedge_counts(dg)
+    ecount = torch.zeros(g.m, dtype=torch.int64, device="cuda")
+    wing = torch.zeros(g.m, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        pb.count_e(dg, WORKLOAD["count_type"], WORKLOAD["rank_type"], use_v=use_v, out=ecount)
+        s1 = ctx.stats()
+        pb.peel_e(dg, ecount, WORKLOAD["peel_type"], use_v=use_v, out=wing)
+        s2 = ctx.stats()
+        return s1, s2
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.kernel_launches()
+    durs, count_ms, peel_ms, agg_ms, stats = [], [], [], [], None
+    torch.cuda.synchronize()
+    barrier(world)
+    for _ in range(args.steps):
+        flush.fill_(1)  # evicts L2 (256 MiB > 126 MiB) outside the timed span
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s1, s2 = step()
+        e1.record(stream)
+        e1.synchronize()
+        durs.append(e0.elapsed_time(e1))
+        count_ms.append(sum(s1[k] for k in ("ms_rank", "ms_relabel", "ms_scan", "ms_count", "ms_convert")))
+        agg_ms.append(s1["ms_agg_kernel"])
+        peel_ms.append(s2["ms_peel"])
+        stats = (s1, s2)
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = ctx.kernel_launches() - launches0
+    clk = clocks.stop()
+    ms_step = max_over_ranks(sum(durs) / len(durs), world)
+    s1, s2 = stats
+    w_rank = int(s1["w_rank"])
+    value = w_rank * world / (ms_step / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers ------------------------------------
+    host = {name: torch.from_numpy(getattr(g, name)).pin_memory() for name in ("offsetsV", "edgesV", "offsetsU", "edgesU")}
+    ec_host = torch.zeros(g.m, dtype=torch.int64).pin_memory()
+    wing_host = torch.zeros(g.m, dtype=torch.int64).pin_memory()
+    from parbutterfly_b200 import _ffi
+    import ctypes as C
+
+    def e2e_step():
+        s = _ffi.CSR(g.nv, g.nu, g.m, host["offsetsV"].data_ptr(), host["edgesV"].data_ptr(),
+                     host["offsetsU"].data_ptr(), host["edgesU"].data_ptr())
+        h = C.c_void_p()
+        ctx.check(ctx._lib.pb_graph_upload(ctx.handle, C.byref(s), C.byref(h)), "pb_graph_upload")
+        o = pb.make_opts(WORKLOAD["count_type"], WORKLOAD["rank_type"], per="EDGE", use_v=use_v)
+        ctx.check(ctx._lib.pb_count_edge(ctx.handle, h, C.byref(o), ec_host.data_ptr()), "pb_count_edge")
+        o2 = pb.make_opts(peel_type=WORKLOAD["peel_type"], per="EDGE", use_v=use_v)
+        ctx.check(ctx._lib.pb_peel_edge(ctx.handle, h, C.byref(o2), ec_host.data_ptr(), wing_host.data_ptr()),
+                  "pb_peel_edge")
+        ctx._lib.pb_graph_destroy(h)
+
+    e2e_steps = max(1, min(args.steps, 2))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, world)
+    assert torch.equal(ec_host, ecount.cpu()) and torch.equal(wing_host, wing.cpu()), "e2e results differ"
+    h2d = g.nbytes + g.m * 8
+    d2h = 2 * g.m * 8
+
+    # ---- roofline of the dominant kernel ------------------------------------------------------------
+    peak, peak_kind = measured_peaks()
+    peel_share = statistics.mean(peel_ms) / (ms_step)
+    n = g.nv + g.nu
+    if peel_share >= 0.5:
+        # wing peeling: 4 B per probed neighbour id (the enumerated two-hop entries)
+        alg_bytes = 4.0 * s2["peel_work"]
+        dur = statistics.mean(peel_ms) / 1e3
+        kern = "peel_kernel<wing> (persistent cooperative wing peeling)"
+    else:
+        alg_bytes = 4.0 * w_rank + 4.0 * (n + 1) + 4.0 * 2 * g.m + 8.0 * g.m
+        dur = statistics.mean(agg_ms) / 1e3
+        kern = "count_warp_kernel + count_block_kernel (wedge aggregation)"
+    achieved = alg_bytes / dur / 1e9
+    agg_bytes = 4.0 * w_rank + 4.0 * (n + 1) + 4.0 * 2 * g.m + 8.0 * g.m
+    agg_gbs = agg_bytes / (statistics.mean(agg_ms) / 1e3) / 1e9
+
+    line = {
+        "metric": "wedges/s", "value": value, "unit": "wedges/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded R-MAT generator)",
+        "config": dict(WORKLOAD, w_rank=w_rank, w_side=w_side, parallelism=f"replicas x{world}"),
+        "count_ms": statistics.mean(count_ms), "peel_ms": statistics.mean(peel_ms),
+        "count_wedges_per_s": w_rank / (statistics.mean(count_ms) / 1e3),
+        "peel_rounds": s2["peel_rounds"], "peel_work": s2["peel_work"],
+        "aggregation": {"ms": statistics.mean(agg_ms), "alg_bytes": agg_bytes, "achieved_gbs": agg_gbs,
+                        "frac": agg_gbs / peak},
+        "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
+        "e2e": {"value": w_rank * world / (e2e_ms / 1e3), "unit": "wedges/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            _, wr_s, times, r = run_cpu_baseline(CPU_SAMPLE, threads)
+            sample = (f"bipartite R-MAT 2^{CPU_SAMPLE['log_nv']} x 2^{CPU_SAMPLE['log_nu']}, m=2^19, same generator "
+                      f"and flags; W_rank={wr_s}; count {r['count_s']:.2f} s + wing peel {r['peel_s']:.2f} s")
+            line["cpu_baseline"] = {"value": wr_s / times[0], "unit": "wedges/s", "cores": threads,
+                                    "kind": "reference", "sample": sample}
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "wedges/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {ex}"}
+    dg.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            our_arm(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

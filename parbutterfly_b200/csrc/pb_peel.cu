@@ -50,15 +50,25 @@ struct Ctl {
   unsigned alen[2];               // alive list lengths
   unsigned hist[66];
   unsigned bar_count, bar_gen, err;
+  unsigned long long round;   // next round to run (kept across launches)
+  unsigned alist_cur;         // current alive list (kept across launches)
+  unsigned started;           // alive list initialised
+  unsigned alive_at_compact;  // unpeeled items when the lists were last compacted
+  unsigned min_gain;          // pause for compaction once this many more items are peeled
 };
 
+// Live adjacency of both sides.  Lists are compacted to their live entries between launches
+// of the peeling kernel, so list positions are not edge ids: eidK / eidC carry the output
+// edge index of every entry.
 struct Lists {
   const uint32_t* offK;  // count side: vertex -> centre ids
   const uint32_t* edgK;
-  const uint32_t* offC;  // centre side: vertex -> count-side ids (positions = output edge index)
+  const uint32_t* eidK;  // count-side entry -> output edge index (wing only)
+  const uint32_t* offC;  // centre side: vertex -> count-side ids
   const uint32_t* edgC;
-  const uint32_t* eti;   // count-side list position -> output edge index (wing only)
+  const uint32_t* eidC;  // centre-side entry -> output edge index (wing only)
   const uint32_t* center_of;  // output edge index -> centre vertex (wing only)
+  const uint32_t* u_of;       // output edge index -> count-side vertex (wing only)
   const int64_t* S;      // per count-side vertex then per centre vertex: sum of neighbour degrees (wing)
   const int64_t* wk;     // per count-side vertex: two-hop wedges sum(deg(v) - 1) (tip)
   int64_t nK, nC;
@@ -378,8 +388,8 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   sync();
   for (uint32_t p = pb + rank; p < pe; p += gsize) {
     uint32_t key, e;
-    if (E.from_v) { key = G.edgK[p]; e = G.eti[p]; }
-    else { key = G.edgC[p]; e = p; }
+    if (E.from_v) { key = G.edgK[p]; e = G.eidK[p]; }
+    else { key = G.edgC[p]; e = G.eidC[p]; }
     if (W.state[e] == PEELED) continue;
     if (hash) t_put(keys, vals, mask, key, e, ctl);
     else mark[key] = e + 1;
@@ -395,13 +405,13 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   PosAcc acc;
   unsigned long long my_work = 0;
   auto flush = [&]() {
-    if (acc.j != kEmpty && acc.acc) dec(W, ctl, par, E.from_v ? acc.j : G.eti[acc.j], acc.acc);
+    if (acc.j != kEmpty && acc.acc) dec(W, ctl, par, E.from_v ? G.eidC[acc.j] : G.eidK[acc.j], acc.acc);
     acc.acc = 0;
   };
   if (E.from_v) {
     auto first = [&](uint32_t p, uint32_t& L, uint32_t& sb) {
       const uint32_t u2 = G.edgC[p];
-      if (u2 == E.u || skip_edge(W, p, E.e1)) { L = 0; sb = 0; return; }
+      if (u2 == E.u || skip_edge(W, G.eidC[p], E.e1)) { L = 0; sb = 0; return; }
       sb = G.offK[u2];
       L = G.offK[u2 + 1] - sb;
     };
@@ -409,7 +419,7 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       ++my_work;
       const uint32_t v2 = G.edgK[q];
       if (v2 == E.v) return;
-      const uint32_t e3 = G.eti[q];
+      const uint32_t e3 = G.eidK[q];
       if (skip_edge(W, e3, E.e1)) return;
       uint32_t e4;
       if (!probe(v2, e4) || (W.state[e4] == ACTIVE && e4 < E.e1)) return;
@@ -423,7 +433,7 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   } else {
     auto first = [&](uint32_t q, uint32_t& L, uint32_t& sb) {
       const uint32_t v2 = G.edgK[q];
-      if (v2 == E.v || skip_edge(W, G.eti[q], E.e1)) { L = 0; sb = 0; return; }
+      if (v2 == E.v || skip_edge(W, G.eidK[q], E.e1)) { L = 0; sb = 0; return; }
       sb = G.offC[v2];
       L = G.offC[v2 + 1] - sb;
     };
@@ -431,11 +441,12 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       ++my_work;
       const uint32_t u2 = G.edgC[p3];
       if (u2 == E.u) return;
-      if (skip_edge(W, p3, E.e1)) return;
+      const uint32_t e3 = G.eidC[p3];
+      if (skip_edge(W, e3, E.e1)) return;
       uint32_t e2;
       if (!probe(u2, e2) || (W.state[e2] == ACTIVE && e2 < E.e1)) return;
       dec(W, ctl, par, e2, 1);
-      dec(W, ctl, par, p3, 1);
+      dec(W, ctl, par, e3, 1);
       if (q != acc.j) { flush(); acc.j = q; }
       acc.acc += 1;
     };
@@ -460,7 +471,7 @@ struct Classify {
     return G.S[G.nK + v] <= G.S[u];
   }
   __device__ __forceinline__ bool wing_small(const Lists& G, uint32_t e) const {
-    const uint32_t v = G.center_of[e], u = G.edgC[e];
+    const uint32_t v = G.center_of[e], u = G.u_of[e];
     const bool fv = wing_from_v(G, v, u);
     const int64_t work = fv ? G.S[G.nK + v] : G.S[u];
     const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
@@ -478,14 +489,28 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
   uint32_t* wvals = wkeys + kWarpSlots;
   const unsigned gtid = blockIdx.x * kPT + threadIdx.x;
   const unsigned gthreads = gridDim.x * kPT;
-  unsigned alist_cur = 0;
+  unsigned alist_cur = *(volatile unsigned*)&ctl->alist_cur;
   unsigned long long work = 0;
-  for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = (uint32_t)x;
-  if (!grid_barrier(ctl)) return;
+  if (!*(volatile unsigned*)&ctl->started) {
+    for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = (uint32_t)x;
+    if (!grid_barrier(ctl)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->started = 1;
+  }
 
-  for (unsigned long long r = 0;; ++r) {
+  for (unsigned long long r = *(volatile unsigned long long*)&ctl->round;; ++r) {
     const unsigned par = (unsigned)(r & 1ull), npar = par ^ 1u;
-    if (*(volatile unsigned*)&ctl->alive == 0) break;
+    const unsigned alive = *(volatile unsigned*)&ctl->alive;
+    if (alive == 0) break;
+    // Pause at a round boundary once enough items have been peeled since the lists were last
+    // compacted; the host compacts them and relaunches (all CTAs see the same values here).
+    const unsigned at_compact = *(volatile unsigned*)&ctl->alive_at_compact;
+    if (2u * alive < at_compact && at_compact - alive >= *(volatile unsigned*)&ctl->min_gain) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->round = r;
+        ctl->alist_cur = alist_cur;
+      }
+      break;
+    }
     unsigned long long k = *(volatile unsigned long long*)&ctl->nm[par];
     if (k == kInf) {
       // ---- window advance (no unpeeled item left in the near list): compact the alive list
@@ -589,11 +614,12 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= ns) break;
         const uint32_t x = W.fsmall[par][q];
+        if (W.cnt[x] == 0) continue;  // no live butterfly contains x: nothing to remove
         if (kWing) {
           WingEdge E;
           E.e1 = x;
           E.v = G.center_of[x];
-          E.u = G.edgC[x];
+          E.u = G.u_of[x];
           E.from_v = cls.wing_from_v(G, E.v, E.u);
           wing_item<false>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work);
         } else {
@@ -609,11 +635,12 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         __syncthreads();
         if (q >= nb) break;
         const uint32_t x = W.fbig[par][q];
+        if (W.cnt[x] == 0) continue;  // uniform across the CTA
         if (kWing) {
           WingEdge E;
           E.e1 = x;
           E.v = G.center_of[x];
-          E.u = G.edgC[x];
+          E.u = G.u_of[x];
           E.from_v = cls.wing_from_v(G, E.v, E.u);
           wing_item<true>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work);
         } else {
@@ -728,48 +755,146 @@ __global__ void max_i64_kernel(const int64_t* __restrict__ a, int64_t n, unsigne
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Live-entry count per vertex.  kByEdge: an entry is live when its edge is not peeled
+// (wing); otherwise when its neighbour (a count-side vertex) is not peeled (tip, centre lists).
+template <bool kByEdge>
+__global__ void live_degree_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                                   const uint32_t* __restrict__ eid, int64_t n, const uint8_t* __restrict__ state,
+                                   uint32_t* deg) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t x = warp; x < n; x += nwarps) {
+    uint32_t c = 0;
+    for (uint32_t p = off[x] + lane; p < off[x + 1]; p += 32)
+      c += state[kByEdge ? eid[p] : nbr[p]] != PEELED;
+    c = warp_sum(c);
+    if (lane == 0) deg[x] = c;
+  }
+}
+
+// Stable filter of every list to its live entries (order kept, so lists stay ascending).
+template <bool kByEdge>
+__global__ void compact_lists_kernel(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                                     const uint32_t* __restrict__ eid, int64_t n, const uint8_t* __restrict__ state,
+                                     const uint32_t* __restrict__ noff, uint32_t* nnbr, uint32_t* neid) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t x = warp; x < n; x += nwarps) {
+    uint32_t dst = noff[x];
+    const uint32_t e = off[x + 1];
+    for (uint32_t p0 = off[x]; p0 < e; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      bool live = false;
+      uint32_t y = 0, id = 0;
+      if (p < e) {
+        y = nbr[p];
+        id = eid ? eid[p] : 0u;
+        live = state[kByEdge ? id : y] != PEELED;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, live);
+      if (live) {
+        const uint32_t at = dst + __popc(bal & ((1u << lane) - 1u));
+        nnbr[at] = y;
+        if (neid) neid[at] = id;
+      }
+      dst += __popc(bal);
+    }
+  }
+}
+
+__global__ void iota_kernel(uint32_t* a, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = (uint32_t)i;
+}
+
 int grid_for(int64_t n, int per_block = 256) { return std::max(1, std::min(ceil_div(n, per_block), sm_count() * 16)); }
+
+// One side's live lists (double-buffered so a compaction can read the previous version).
+struct LiveSide {
+  DevBuf<uint32_t> off[2], nbr[2], eid[2];
+  int cur = 0;
+  int64_t n = 0;
+};
+
+template <bool kByEdge>
+void compact_side(LiveSide& L, const uint32_t* off, const uint32_t* nbr, const uint32_t* eid, const uint8_t* state,
+                  bool with_eid, cudaStream_t s) {
+  const int nx = L.cur ^ 1;
+  DevBuf<uint32_t> deg(L.n > 0 ? L.n : 1, s);
+  if (L.n) PB_LAUNCH(live_degree_kernel<kByEdge>, grid_for(L.n * 32), 256, 0, s, off, nbr, eid, L.n, state, deg.get());
+  if (L.off[nx].n < (size_t)L.n + 1) L.off[nx].alloc(L.n + 1, s);
+  exclusive_scan_u32(deg.get(), L.off[nx].get(), L.n, s);
+  uint32_t live = 0;
+  PB_CUDA_TRY(cudaMemcpyAsync(&live, L.off[nx].get() + L.n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  if (L.nbr[nx].n < (size_t)live + 1) L.nbr[nx].alloc(live + 1, s);
+  if (with_eid && L.eid[nx].n < (size_t)live + 1) L.eid[nx].alloc(live + 1, s);
+  if (L.n)
+    PB_LAUNCH(compact_lists_kernel<kByEdge>, grid_for(L.n * 32), 256, 0, s, off, nbr, with_eid ? eid : nullptr, L.n,
+              state, L.off[nx].get(), L.nbr[nx].get(), with_eid ? L.eid[nx].get() : nullptr);
+  L.cur = nx;
+}
 
 template <bool kWing>
 PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t* out, cudaStream_t s) {
   PeelResult res;
   Lists G{};
-  G.offK = use_v ? g.offU.get() : g.offV.get();
-  G.edgK = use_v ? g.edgU.get() : g.edgV.get();
-  G.offC = use_v ? g.offV.get() : g.offU.get();
-  G.edgC = use_v ? g.edgV.get() : g.edgU.get();
+  const uint32_t* offK0 = use_v ? g.offU.get() : g.offV.get();
+  const uint32_t* edgK0 = use_v ? g.edgU.get() : g.edgV.get();
+  const uint32_t* offC0 = use_v ? g.offV.get() : g.offU.get();
+  const uint32_t* edgC0 = use_v ? g.edgV.get() : g.edgU.get();
   G.nK = use_v ? g.nu : g.nv;
   G.nC = use_v ? g.nv : g.nu;
   const int64_t N = kWing ? g.m : G.nK;
   if (N == 0) return res;
   PB_REQUIRE(N < (int64_t)UINT32_MAX, PB_ETOOBIG, "too many items to peel");
+  G.offK = offK0;
+  G.edgK = edgK0;
+  G.offC = offC0;
+  G.edgC = edgC0;
 
   DevBuf<int64_t> cnt(N, s), wk, Sx;
-  DevBuf<uint32_t> eti, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
+  DevBuf<uint32_t> eti, iota, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
   DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), tl0(N, s), tl1(N, s);
   DevBuf<uint8_t> state(N, s), in_near(N, s);
+  LiveSide liveK, liveC;
+  liveK.n = G.nK;
+  liveC.n = G.nC;
   PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, out, cnt.get(), state.get(), in_near.get(),
             touched.get());
+  auto refresh_work = [&]() {
+    if (kWing) {
+      if (G.nK) PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, Sx.get());
+      if (G.nC)
+        PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.edgC, G.offK, G.nC, Sx.get() + G.nK);
+    } else {
+      PB_LAUNCH(tip_work_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, wk.get());
+    }
+  };
   bool need_scratch = false;
   int64_t scratch_len = 0;
   if (kWing) {
     eti.alloc(g.m, s);
+    iota.alloc(g.m, s);
     center_of.alloc(g.m, s);
     Sx.alloc(G.nK + G.nC, s);
     edge_to_idxs(g, use_v, eti.get(), s);
+    PB_LAUNCH(iota_kernel, grid_for(g.m), 256, 0, s, iota.get(), g.m);
     PB_LAUNCH(center_of_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.nC, center_of.get());
-    if (G.nK) PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, Sx.get());
-    if (G.nC)
-      PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.edgC, G.offK, G.nC, Sx.get() + G.nK);
-    G.eti = eti.get();
+    G.eidK = eti.get();
+    G.eidC = iota.get();
     G.center_of = center_of.get();
+    G.u_of = edgC0;  // edge ids are positions in the centre side's original lists
     G.S = Sx.get();
+    refresh_work();
     need_scratch = 2ull * g.max_deg > (uint64_t)kBlockSlots;
     scratch_len = std::max(G.nK, G.nC);
   } else {
     wk.alloc(G.nK, s);
-    PB_LAUNCH(tip_work_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, wk.get());
     G.wk = wk.get();
+    refresh_work();
     DevBuf<unsigned long long> mx(1, s);
     PB_CUDA_TRY(cudaMemsetAsync(mx.get(), 0, sizeof(unsigned long long), s));
     PB_LAUNCH(max_i64_kernel, grid_for(G.nK), 256, 0, s, wk.get(), G.nK, mx.get());
@@ -819,18 +944,43 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.k_lo = kInf;
   hctl.alive = (unsigned)N;
   hctl.alen[0] = (unsigned)N;
+  hctl.alive_at_compact = (unsigned)N;
+  hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
   DevBuf<Ctl> ctl(1, s);
   PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
   Classify cls{8192};
   Ctl* ctl_ptr = ctl.get();
-  void* args[] = {&G, &W, &ctl_ptr, &cls};
-  PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
-  if (g_launch_counter) ++*g_launch_counter;
-  PB_CUDA_TRY(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(Ctl), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
-  PB_REQUIRE(!(hctl.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
-  PB_REQUIRE(hctl.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
-  PB_REQUIRE(hctl.alive == 0, PB_ECUDA, "peeling ended with unpeeled items");
+  int launches = 0;
+  while (true) {
+    void* args[] = {&G, &W, &ctl_ptr, &cls};
+    PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
+    if (g_launch_counter) ++*g_launch_counter;
+    ++launches;
+    PB_CUDA_TRY(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    PB_REQUIRE(!(hctl.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
+    PB_REQUIRE(hctl.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
+    if (hctl.alive == 0) break;
+    PB_REQUIRE(launches < 4096, PB_ECUDA, "peeling: too many relaunches");
+    // Compact the lists to their live entries and resume.
+    if (kWing) {
+      compact_side<true>(liveK, G.offK, G.edgK, G.eidK, state.get(), true, s);
+      compact_side<true>(liveC, G.offC, G.edgC, G.eidC, state.get(), true, s);
+      G.offK = liveK.off[liveK.cur].get();
+      G.edgK = liveK.nbr[liveK.cur].get();
+      G.eidK = liveK.eid[liveK.cur].get();
+      G.offC = liveC.off[liveC.cur].get();
+      G.edgC = liveC.nbr[liveC.cur].get();
+      G.eidC = liveC.eid[liveC.cur].get();
+    } else {
+      compact_side<false>(liveC, G.offC, G.edgC, nullptr, state.get(), false, s);
+      G.offC = liveC.off[liveC.cur].get();
+      G.edgC = liveC.nbr[liveC.cur].get();
+    }
+    refresh_work();
+    const unsigned alive = hctl.alive;
+    PB_CUDA_TRY(cudaMemcpyAsync(&ctl.get()->alive_at_compact, &alive, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  }
   res.rounds = (int64_t)hctl.rounds;
   res.work = (int64_t)hctl.work;
   return res;
