@@ -153,6 +153,23 @@ pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, cons
 pb_status pb_peel_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* ecounts,
                        int64_t* wing);
 
+/* ---- counting without device allocation ------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc where they need a
+ * count (code running inside another framework's memory pool, paths that must not synchronise
+ * the device, callers close to the memory limit): total butterflies of a graph whose four CSR
+ * arrays are already in device memory, written to *total (device memory), on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  Nothing is allocated: all scratch lives in one
+ * file-scope device array of PB_NOALLOC_SCRATCH_BYTES, reserved on every GPU that loads the
+ * library until the process exits.  Limit: max(nv, nu) <= PB_NOALLOC_MAX_SIDE, else PB_ETOOBIG
+ * (message in msg when msg_len > 0).  The graph must satisfy pb_graph_upload's contract; it is
+ * not validated.  The first call on a device resolves the array's device address with that
+ * device current; make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race and give wrong
+ * results.  Asynchronous: *total is ready when `stream` reaches this point. */
+#define PB_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define PB_NOALLOC_MAX_SIDE ((1u << 22) - 64u)
+pb_status pb_count_total_noalloc(const pb_csr* dev_graph, void* stream, int64_t* total, char* msg, size_t msg_len);
+
 /* ---- host utilities (no GPU needed) ---------------------------------------------------- */
 void pb_csr_free(pb_csr_owned* g);
 /* readBipartite (butterfly_utils.h:1008-1058): Ligra "AdjacencyHypergraph" text file. */

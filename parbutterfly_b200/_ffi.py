@@ -24,7 +24,7 @@ EXPORTS = [
     "pb_graph_dims", "pb_cmp_wedge_counts", "pb_edge_to_idxs", "pb_count_vert", "pb_count_edge",
     "pb_count_total", "pb_peel_vert", "pb_peel_edge", "pb_csr_free", "pb_read_adjacency_hypergraph",
     "pb_write_adjacency_hypergraph", "pb_csr_validate", "pb_gen_uniform", "pb_gen_rmat",
-    "pb_gen_powerlaw_u", "pb_gen_zipf", "pb_gen_batch_member",
+    "pb_gen_powerlaw_u", "pb_gen_zipf", "pb_gen_batch_member", "pb_count_total_noalloc",
 ]
 
 
@@ -106,6 +106,7 @@ def lib():
         "pb_gen_powerlaw_u": (S, [I64, I64, I64, D, I64, U64, C.POINTER(CSR)]),
         "pb_gen_zipf": (S, [I64, I64, I64, D, U64, C.POINTER(CSR)]),
         "pb_gen_batch_member": (S, [I32, C.POINTER(CSR)]),
+        "pb_count_total_noalloc": (S, [C.POINTER(CSR), P, P, C.c_char_p, C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         try:
