@@ -19,6 +19,8 @@
 // pass over the alive list, a log2 histogram of distances to the minimum) when the near list
 // runs dry.  Frontier items with little work run one per warp; heavy ones one per CTA.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "pb_engine.cuh"
@@ -29,9 +31,8 @@ namespace pb {
 namespace {
 
 constexpr int kPT = 512;
-constexpr int kPW = kPT / 32;
-constexpr int kWarpSlots = 1024;   // per-warp table slots (keys + values: 8 KiB)
-constexpr int kBlockSlots = 16384; // per-CTA table slots (128 KiB), shares memory with warp tables
+constexpr int kWarpSlots = 512;    // per-warp table slots (keys + values: 4 KiB)
+constexpr int kBlockSlots = 8192;  // per-CTA table slots (64 KiB), shares memory with warp tables
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kInf = ~0ull;
 constexpr uint8_t ALIVE = 0, ACTIVE = 1, PEELED = 2;
@@ -42,9 +43,11 @@ struct Ctl {
   unsigned long long nm[2];       // next minimum per round parity
   unsigned long long k_lo, win_hi;
   unsigned long long rounds, work;
-  unsigned flen_small[2], flen_big[2];
+  unsigned flen_small[2], flen_big[2], flen_huge[2];
   unsigned tlen[2];
   unsigned cur_small[2], cur_big[2];
+  unsigned units;  // work units (chunks of CTA-level items) of the current round
+  unsigned long long round_cost[2];  // summed cost estimate of the round's CTA-level items
   unsigned near_len;
   unsigned alive;                 // unpeeled items
   unsigned alen[2];               // alive list lengths
@@ -55,7 +58,11 @@ struct Ctl {
   unsigned started;           // alive list initialised
   unsigned alive_at_compact;  // unpeeled items when the lists were last compacted
   unsigned min_gain;          // pause for compaction once this many more items are peeled
+  // Instrumentation (CTA 0): device time per phase and work counters.
+  unsigned long long t_last, phase_ns[4];  // advance, F, P, U
+  unsigned long long scanned, touched_total, n_small, n_big, n_huge, advances;
 };
+
 
 // Live adjacency of both sides.  Lists are compacted to their live entries between launches
 // of the peeling kernel, so list positions are not edge ids: eidK / eidC carry the output
@@ -84,7 +91,11 @@ struct Work {
   uint32_t* near;
   uint32_t* fsmall[2];
   uint32_t* fbig[2];
+  uint32_t* fchunks[2];  // work units of each CTA-level item (parallel to fbig)
+  uint32_t* uprefix;     // exclusive prefix of fchunks for the current round (N + 1)
+  uint32_t* fhuge[2];
   uint32_t* tlist[2];
+  uint32_t* gshared;   // grid-shared dense counters / probe markers for huge items (zeroed)
   uint32_t* gscratch;  // per-CTA dense scratch (dense counters / probe markers)
   int64_t gscratch_len;
   int64_t N;           // items
@@ -94,6 +105,15 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// CTA 0 charges the time since its previous mark to phase `ph` (called right after barriers).
+__device__ __forceinline__ void phase_mark(Ctl* ctl, int ph) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long now = globaltimer_ns();
+    if (ctl->t_last) ctl->phase_ns[ph] += now - ctl->t_last;
+    ctl->t_last = now;
+  }
 }
 
 // Grid barrier for a cooperative launch (all CTAs co-resident).  Bounded: a wait longer than
@@ -120,7 +140,6 @@ __device__ bool grid_barrier(Ctl* ctl) {
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
     __threadfence();
@@ -260,14 +279,75 @@ __device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, Fi
   }
 }
 
+// The same iteration restricted to flattened pair indices [lo, hi) (counted from the first
+// pair of [b, e)); every CTA of the grid takes one slice of a huge item.
+template <class First, class F>
+__device__ __forceinline__ void block_iter_range(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f,
+                                                 uint64_t lo, uint64_t hi) {
+  const uint32_t tid = threadIdx.x;
+  uint64_t base = 0;
+  for (uint32_t j0 = b; j0 < e && base < hi; j0 += kPT) {
+    const uint32_t j = j0 + tid;
+    uint32_t L = 0, sb = 0;
+    if (j < e) first(j, L, sb);
+    uint32_t T;
+    const uint32_t incl = block_incl_scan(L, S.scan, T);
+    S.incl[tid] = incl;
+    S.sb[tid] = sb;
+    __syncthreads();
+    const uint64_t tb = lo > base ? lo - base : 0;
+    const uint64_t te = (hi - base) < (uint64_t)T ? (hi - base) : (uint64_t)T;
+    for (uint64_t t0 = tb; t0 < te; t0 += kPT) {
+      const uint64_t tt = t0 + tid;
+      if (tt < te) {
+        const uint32_t t = (uint32_t)tt;
+        uint32_t lo2 = 0;
+#pragma unroll
+        for (uint32_t step = kPT / 2; step > 0; step >>= 1)
+          if (S.incl[lo2 + step - 1] <= t) lo2 += step;
+        const uint32_t ex = lo2 ? S.incl[lo2 - 1] : 0u;
+        f(j0 + lo2, S.sb[lo2] + (t - ex));
+      }
+    }
+    __syncthreads();
+    base += T;
+  }
+}
+
+// Sum of the second-level lengths of [b, e) (valid in every thread).
+template <class First>
+__device__ __forceinline__ uint64_t block_total(uint32_t b, uint32_t e, Shared& S, First&& first) {
+  unsigned long long sum = 0;
+  for (uint32_t j = b + threadIdx.x; j < e; j += kPT) {
+    uint32_t L = 0, sb = 0;
+    first(j, L, sb);
+    sum += L;
+  }
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  unsigned long long t = 0;
+  for (int w = 0; w < kPT / 32; ++w) t += S.red[w];
+  __syncthreads();
+  return t;
+}
+
 __device__ __forceinline__ void touch(const Work& W, Ctl* ctl, unsigned par, uint32_t x) {
   if (W.touched[x] == 0 && atomicExch(&W.touched[x], 1u) == 0u) W.tlist[par][atomicAdd(&ctl->tlen[par], 1u)] = x;
 }
 
+// Window bound of the current round, per CTA (set at the start of every round).
+__shared__ unsigned long long s_win_hi;
+
+// Removes `amount` butterflies from an unpeeled item.  Only an item whose count falls below
+// the window bound can reach the frontier before the next window advance, so only those are
+// queued for re-bucketing; items that stay above it keep bucket == count implicitly (the
+// advance resynchronises buckets from counts, when no unpeeled item is in the near list).
 __device__ __forceinline__ void dec(const Work& W, Ctl* ctl, unsigned par, uint32_t x, int64_t amount) {
   if (W.state[x] == ALIVE) {
-    atomic_add_i64(&W.cnt[x], -amount);
-    touch(W, ctl, par, x);
+    const long long old = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&W.cnt[x]),
+                                               (unsigned long long)(-amount));
+    if ((unsigned long long)(old - amount) < s_win_hi) touch(W, ctl, par, x);
   }
 }
 
@@ -355,6 +435,13 @@ __device__ void tip_item_block(const Lists& G, const Work& W, Ctl* ctl, unsigned
 // (u2, edge e2), second level N(u2) (v2, edge e3), probe v2 -> e4.
 // Orientation B (walk from u): probe set N(v) (count-side vertex -> edge), first level N(u)
 // (v2, e4), second level N(v2) (u2, e3), probe u2 -> e2.  Both find the same butterflies.
+constexpr uint32_t kRevFlag = 0x80000000u;  // list positions stay below 2^31 (2m <= 2^32)
+
+// Binary-searching a list of length dbig for each of dsmall keys beats scanning it.
+__device__ __forceinline__ bool reverse_cheaper(uint32_t dsmall, uint32_t dbig) {
+  return (uint64_t)dsmall * (uint64_t)(33u - __clz(dbig | 1u)) < (uint64_t)dbig;
+}
+
 struct WingEdge {
   uint32_t e1, u, v;
   bool from_v;
@@ -365,27 +452,32 @@ __device__ __forceinline__ bool skip_edge(const Work& W, uint32_t e, uint32_t e1
   return s == PEELED || (s == ACTIVE && e < e1);
 }
 
-template <bool kBlockLevel>
-__device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par, const WingEdge& E, uint32_t* keys,
-                          uint32_t* vals, uint32_t slots, Shared* S, unsigned long long& work) {
-  const uint32_t rank = kBlockLevel ? threadIdx.x : lane_id();
-  const uint32_t gsize = kBlockLevel ? kPT : 32;
-  auto sync = [&]() {
-    if (kBlockLevel) __syncthreads();
-    else __syncwarp();
+// Item granularity: one warp, one CTA, or the whole grid (huge items; all CTAs call it).
+enum Level { LV_WARP = 0, LV_BLOCK = 1, LV_GRID = 2 };
+
+template <int kLevel>
+__device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par, const WingEdge& E, uint32_t* keys,
+                          uint32_t* vals, uint32_t slots, Shared* S, unsigned long long& work, uint32_t chunk = 0,
+                          uint32_t nchunks = 1) {
+  const uint32_t rank = kLevel == LV_WARP ? lane_id() : (kLevel == LV_GRID ? blockIdx.x * kPT + threadIdx.x : threadIdx.x);
+  const uint32_t gsize = kLevel == LV_WARP ? 32 : (kLevel == LV_GRID ? gridDim.x * kPT : kPT);
+  auto sync = [&]() -> bool {
+    if (kLevel == LV_WARP) { __syncwarp(); return true; }
+    if (kLevel == LV_BLOCK) { __syncthreads(); return true; }
+    return grid_barrier(ctl);
   };
-  // probe set
+  // Probe set: N(u) (keys: centres) when walking from v, else N(v) (keys: count-side ids).
   uint32_t pb, pe;
   if (E.from_v) { pb = G.offK[E.u]; pe = G.offK[E.u + 1]; }
   else { pb = G.offC[E.v]; pe = G.offC[E.v + 1]; }
   const uint32_t psize = pe - pb;
-  const bool hash = 2 * psize <= slots;
-  uint32_t* mark = W.gscratch + (size_t)blockIdx.x * (size_t)W.gscratch_len;
+  const bool hash = kLevel != LV_GRID && 2 * psize <= slots;
+  uint32_t* mark = kLevel == LV_GRID ? W.gshared : W.gscratch + (size_t)blockIdx.x * (size_t)W.gscratch_len;
   const uint32_t tsize = hash ? max(64u, np2(2u * psize)) : 0u;
   const uint32_t mask = tsize - 1;
   if (hash)
     for (uint32_t s = rank; s < tsize; s += gsize) keys[s] = kEmpty;
-  sync();
+  if (!sync()) return false;
   for (uint32_t p = pb + rank; p < pe; p += gsize) {
     uint32_t key, e;
     if (E.from_v) { key = G.edgK[p]; e = G.eidK[p]; }
@@ -394,7 +486,7 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     if (hash) t_put(keys, vals, mask, key, e, ctl);
     else mark[key] = e + 1;
   }
-  sync();
+  if (!sync()) return false;
   auto probe = [&](uint32_t key, uint32_t& e) -> bool {
     if (hash) return t_get(keys, vals, mask, key, e);
     const uint32_t x = mark[key];
@@ -408,74 +500,181 @@ __device__ void wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     if (acc.j != kEmpty && acc.acc) dec(W, ctl, par, E.from_v ? G.eidC[acc.j] : G.eidK[acc.j], acc.acc);
     acc.acc = 0;
   };
+  // Each (first-level vertex x, probe set) intersection runs in one of two directions: scan
+  // N(x) and probe the probe-set table, or (when the probe set is much shorter than N(x))
+  // walk the probe set and binary-search N(x), which is sorted.  The direction rides in the
+  // top bit of the second-level position.
+  auto found = [&](uint32_t j, uint32_t ea, uint32_t eb) {
+    dec(W, ctl, par, ea, 1);
+    dec(W, ctl, par, eb, 1);
+    if (j != acc.j) { flush(); acc.j = j; }
+    acc.acc += 1;
+  };
+  auto run = [&](uint32_t b, uint32_t e, auto&& first, auto&& f) {
+    if (kLevel == LV_WARP) {
+      warp_iter(b, e, first, f);
+    } else if (kLevel == LV_BLOCK) {
+      block_iter(b, e, *S, first, f);
+    } else {
+      const uint64_t T = block_total(b, e, *S, first);
+      const uint64_t lo = T * blockIdx.x / gridDim.x, hi = T * (blockIdx.x + 1) / gridDim.x;
+      block_iter_range(b, e, *S, first, f, lo, hi);
+    }
+  };
   if (E.from_v) {
     auto first = [&](uint32_t p, uint32_t& L, uint32_t& sb) {
       const uint32_t u2 = G.edgC[p];
       if (u2 == E.u || skip_edge(W, G.eidC[p], E.e1)) { L = 0; sb = 0; return; }
-      sb = G.offK[u2];
-      L = G.offK[u2 + 1] - sb;
+      const uint32_t b2 = G.offK[u2], d2 = G.offK[u2 + 1] - b2;
+      if (reverse_cheaper(psize, d2)) { sb = pb | kRevFlag; L = psize; }
+      else { sb = b2; L = d2; }
     };
     auto f = [&](uint32_t p, uint32_t q) {
       ++my_work;
+      if (q & kRevFlag) {  // walk N(u), binary-search N(u2)
+        const uint32_t pos = q & ~kRevFlag;
+        const uint32_t v2 = G.edgK[pos];
+        if (v2 == E.v) return;
+        const uint32_t e4 = G.eidK[pos];
+        if (skip_edge(W, e4, E.e1)) return;
+        const uint32_t u2 = G.edgC[p];
+        const uint32_t hi = G.offK[u2 + 1];
+        const uint32_t at = lower_bound_u32(G.edgK, G.offK[u2], hi, v2);
+        if (at == hi || G.edgK[at] != v2) return;
+        const uint32_t e3 = G.eidK[at];
+        if (skip_edge(W, e3, E.e1)) return;
+        found(p, e3, e4);
+        return;
+      }
       const uint32_t v2 = G.edgK[q];
       if (v2 == E.v) return;
-      const uint32_t e3 = G.eidK[q];
-      if (skip_edge(W, e3, E.e1)) return;
       uint32_t e4;
-      if (!probe(v2, e4) || (W.state[e4] == ACTIVE && e4 < E.e1)) return;
-      dec(W, ctl, par, e3, 1);
-      dec(W, ctl, par, e4, 1);
-      if (p != acc.j) { flush(); acc.j = p; }
-      acc.acc += 1;
+      if (!probe(v2, e4)) return;  // most probes miss: test the table before any global read
+      const uint32_t e3 = G.eidK[q];
+      if (skip_edge(W, e3, E.e1) || (W.state[e4] == ACTIVE && e4 < E.e1)) return;
+      found(p, e3, e4);
     };
-    if (kBlockLevel) block_iter(G.offC[E.v], G.offC[E.v + 1], *S, first, f);
-    else warp_iter(G.offC[E.v], G.offC[E.v + 1], first, f);
+    const uint32_t b1 = G.offC[E.v], d1 = G.offC[E.v + 1] - b1;
+    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * (chunk + 1) / nchunks), first, f);
   } else {
     auto first = [&](uint32_t q, uint32_t& L, uint32_t& sb) {
       const uint32_t v2 = G.edgK[q];
       if (v2 == E.v || skip_edge(W, G.eidK[q], E.e1)) { L = 0; sb = 0; return; }
-      sb = G.offC[v2];
-      L = G.offC[v2 + 1] - sb;
+      const uint32_t b2 = G.offC[v2], d2 = G.offC[v2 + 1] - b2;
+      if (reverse_cheaper(psize, d2)) { sb = pb | kRevFlag; L = psize; }
+      else { sb = b2; L = d2; }
     };
     auto f = [&](uint32_t q, uint32_t p3) {
       ++my_work;
+      if (p3 & kRevFlag) {  // walk N(v), binary-search N(v2)
+        const uint32_t pos = p3 & ~kRevFlag;
+        const uint32_t u2 = G.edgC[pos];
+        if (u2 == E.u) return;
+        const uint32_t e2 = G.eidC[pos];
+        if (skip_edge(W, e2, E.e1)) return;
+        const uint32_t v2 = G.edgK[q];
+        const uint32_t hi = G.offC[v2 + 1];
+        const uint32_t at = lower_bound_u32(G.edgC, G.offC[v2], hi, u2);
+        if (at == hi || G.edgC[at] != u2) return;
+        const uint32_t e3 = G.eidC[at];
+        if (skip_edge(W, e3, E.e1)) return;
+        found(q, e2, e3);
+        return;
+      }
       const uint32_t u2 = G.edgC[p3];
       if (u2 == E.u) return;
-      const uint32_t e3 = G.eidC[p3];
-      if (skip_edge(W, e3, E.e1)) return;
       uint32_t e2;
-      if (!probe(u2, e2) || (W.state[e2] == ACTIVE && e2 < E.e1)) return;
-      dec(W, ctl, par, e2, 1);
-      dec(W, ctl, par, e3, 1);
-      if (q != acc.j) { flush(); acc.j = q; }
-      acc.acc += 1;
+      if (!probe(u2, e2)) return;
+      const uint32_t e3 = G.eidC[p3];
+      if (skip_edge(W, e3, E.e1) || (W.state[e2] == ACTIVE && e2 < E.e1)) return;
+      found(q, e2, e3);
     };
-    if (kBlockLevel) block_iter(G.offK[E.u], G.offK[E.u + 1], *S, first, f);
-    else warp_iter(G.offK[E.u], G.offK[E.u + 1], first, f);
+    const uint32_t b1 = G.offK[E.u], d1 = G.offK[E.u + 1] - b1;
+    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * (chunk + 1) / nchunks), first, f);
   }
   flush();
   work += my_work;
-  sync();
+  if (!sync()) return false;
   if (!hash) {  // clear the dense markers
     for (uint32_t p = pb + rank; p < pe; p += gsize) mark[E.from_v ? G.edgK[p] : G.edgC[p]] = 0;
   }
-  sync();
+  return sync();
+}
+
+// Huge tip item: every CTA aggregates one slice of u's two-hop list into grid-shared dense
+// counters; a second pass reads and clears them (atomicExch), crediting each distinct u2 once.
+__device__ bool tip_item_grid(const Lists& G, const Work& W, Ctl* ctl, unsigned par, uint32_t u, Shared& S,
+                              unsigned long long& work) {
+  auto first = [&](uint32_t j, uint32_t& L, uint32_t& sb) {
+    const uint32_t v = G.edgK[j];
+    sb = G.offC[v];
+    L = G.offC[v + 1] - sb;
+  };
+  const uint64_t T = (uint64_t)G.wk[u] + (G.offK[u + 1] - G.offK[u]);
+  const uint64_t lo = T * blockIdx.x / gridDim.x, hi = T * (blockIdx.x + 1) / gridDim.x;
+  uint32_t* cnt = W.gshared;
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+    const uint32_t u2 = G.edgC[q];
+    if (u2 != u) atomicAdd(&cnt[u2], 1u);
+  }, lo, hi);
+  if (!grid_barrier(ctl)) return false;
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+    const uint32_t u2 = G.edgC[q];
+    if (u2 == u) return;
+    const int64_t w = atomicExch(&cnt[u2], 0u);
+    if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
+  }, lo, hi);
+  if (blockIdx.x == 0 && threadIdx.x == 0) work += T;
+  return grid_barrier(ctl);
 }
 
 // ---- the persistent kernel ------------------------------------------------------------------
 // Wing items run on one warp when their work is small and their probe set fits a warp table.
 struct Classify {
   int64_t small_work;
-  __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const { return G.wk[u] <= 512; }
+  int64_t huge_work;   // items above this run on the whole grid
+  int64_t chunk_work;  // target probes per work unit of a CTA-level wing item
+
+  __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const {
+    return G.wk[u] <= kWarpSlots / 2 && G.wk[u] <= small_work;
+  }
+  // Estimated probes from each side: the two-hop list sizes, capped by deg(u)*deg(v) times a
+  // binary-search factor (the reverse-direction intersections).
+  __device__ __forceinline__ int64_t cost_v(const Lists& G, uint32_t v, uint32_t u) const {
+    const int64_t du = G.offK[u + 1] - G.offK[u], dv = G.offC[v + 1] - G.offC[v];
+    return min(G.S[G.nK + v], du * dv * 16);
+  }
+  __device__ __forceinline__ int64_t cost_u(const Lists& G, uint32_t v, uint32_t u) const {
+    const int64_t du = G.offK[u + 1] - G.offK[u], dv = G.offC[v + 1] - G.offC[v];
+    return min(G.S[u], du * dv * 16);
+  }
   __device__ __forceinline__ bool wing_from_v(const Lists& G, uint32_t v, uint32_t u) const {
-    return G.S[G.nK + v] <= G.S[u];
+    return cost_v(G, v, u) <= cost_u(G, v, u);
   }
   __device__ __forceinline__ bool wing_small(const Lists& G, uint32_t e) const {
     const uint32_t v = G.center_of[e], u = G.u_of[e];
     const bool fv = wing_from_v(G, v, u);
-    const int64_t work = fv ? G.S[G.nK + v] : G.S[u];
+    const int64_t work = fv ? cost_v(G, v, u) : cost_u(G, v, u);
     const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
     return work <= small_work && 2 * psize <= (uint32_t)kWarpSlots;
+  }
+  __device__ __forceinline__ bool tip_huge(const Lists& G, uint32_t u) const { return G.wk[u] > huge_work; }
+  // Work units of a CTA-level wing item: first-level slices of at least max(chunk_work,
+  // 4 x probe set) estimated probes each (every unit rebuilds the probe table).
+  __device__ __forceinline__ uint32_t wing_chunks(const Lists& G, uint32_t e) const {
+    const uint32_t v = G.center_of[e], u = G.u_of[e];
+    const bool fv = wing_from_v(G, v, u);
+    const int64_t work = fv ? cost_v(G, v, u) : cost_u(G, v, u);
+    const int64_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
+    const int64_t d1 = fv ? G.offC[v + 1] - G.offC[v] : G.offK[u + 1] - G.offK[u];
+    const int64_t c = max(chunk_work, 4 * psize);
+    int64_t k = (work + c - 1) / c;
+    k = min(k, min(d1, (int64_t)4096));
+    return (uint32_t)max(k, (int64_t)1);
+  }
+  __device__ __forceinline__ bool wing_huge(const Lists& G, uint32_t e) const {
+    const uint32_t v = G.center_of[e], u = G.u_of[e];
+    return min(cost_v(G, v, u), cost_u(G, v, u)) > huge_work;
   }
 };
 
@@ -523,7 +722,11 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         const uint32_t x = W.alist[alist_cur][q];
         if (W.state[x] != ALIVE) continue;
         W.alist[na][atomicAdd(&ctl->alen[na], 1u)] = x;
-        mn = min(mn, (unsigned long long)W.D[x]);
+        // No unpeeled item is in the near list here, and items outside it were queued only
+        // when they fell below the bound: their bucket is their count.
+        const int64_t c = W.cnt[x];
+        W.D[x] = c;
+        mn = min(mn, (unsigned long long)c);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
@@ -571,9 +774,13 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       }
       alist_cur = na;
       if (!grid_barrier(ctl)) return;
+      phase_mark(ctl, 0);
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->advances += 1;
       k = klo;
     }
     const unsigned long long win_hi = *(volatile unsigned long long*)&ctl->win_hi;
+    if (threadIdx.x == 0) s_win_hi = win_hi;
+    __syncthreads();
     // ---- phase F: the frontier is every near item in bucket k; the minimum of the other near
     // items is the first part of the next round's minimum.
     {
@@ -585,9 +792,30 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         const unsigned long long d = (unsigned long long)W.D[x];
         if (d == k) {
           W.state[x] = ACTIVE;
-          const bool small = kWing ? cls.wing_small(G, x) : cls.tip_small(G, x);
+          bool small, huge;
+          int64_t cost;
+          if (kWing) {
+            const uint32_t v = G.center_of[x], u = G.u_of[x];
+            const int64_t cv = cls.cost_v(G, v, u), cu = cls.cost_u(G, v, u);
+            const bool fv = cv <= cu;
+            cost = fv ? cv : cu;
+            const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
+            small = cost <= cls.small_work && 2 * psize <= (uint32_t)kWarpSlots;
+            huge = !small && cost > cls.huge_work;
+          } else {
+            cost = G.wk[x];
+            small = cls.tip_small(G, x);
+            huge = !small && cls.tip_huge(G, x);
+          }
           if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
-          else W.fbig[par][atomicAdd(&ctl->flen_big[par], 1u)] = x;
+          else if (huge) W.fhuge[par][atomicAdd(&ctl->flen_huge[par], 1u)] = x;
+          else {
+            const unsigned at = atomicAdd(&ctl->flen_big[par], 1u);
+            W.fbig[par][at] = x;
+            const int64_t c = cost < 1 ? 1 : (cost > 0x7fffffff ? 0x7fffffff : cost);
+            W.fchunks[par][at] = (uint32_t)c;  // cost for now; CTA 0 turns it into a unit count
+            atomicAdd(&ctl->round_cost[par], (unsigned long long)c);
+          }
         } else {
           mn = min(mn, d);
         }
@@ -598,12 +826,16 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       if (blockIdx.x == 0 && threadIdx.x == 0) {  // slots of the previous round, no longer read
         ctl->flen_small[npar] = 0;
         ctl->flen_big[npar] = 0;
+        ctl->flen_huge[npar] = 0;
+        ctl->round_cost[npar] = 0;
         ctl->tlen[npar] = 0;
         ctl->cur_small[npar] = 0;
         ctl->cur_big[npar] = 0;
+        ctl->scanned += nl;
       }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 1);
     // ---- phase P: process the frontier (small items per warp, then heavy items per CTA).
     {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl->nm[par] = kInf;  // every CTA has read it
@@ -621,34 +853,116 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
           E.v = G.center_of[x];
           E.u = G.u_of[x];
           E.from_v = cls.wing_from_v(G, E.v, E.u);
-          wing_item<false>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work);
+          wing_item<LV_WARP>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work);
         } else {
           tip_item_warp(G, W, ctl, par, x, wkeys, wvals, work);
         }
       }
       __syncthreads();  // warp tables and the CTA table share memory
       const unsigned nb = *(volatile unsigned*)&ctl->flen_big[par];
-      while (true) {
-        if (threadIdx.x == 0) S.item = atomicAdd(&ctl->cur_big[par], 1u);
-        __syncthreads();
-        const unsigned q = S.item;
-        __syncthreads();
-        if (q >= nb) break;
-        const uint32_t x = W.fbig[par][q];
-        if (W.cnt[x] == 0) continue;  // uniform across the CTA
+      if (nb) {
+        // Units: CTA 0 lays out the exclusive prefix of the items' unit counts; every CTA then
+        // pulls units (item, slice) from a shared cursor.
+        if (blockIdx.x == 0) {
+          uint32_t carry = 0;
+          // Unit size: about four units per CTA over the round's CTA-level work, never below
+          // cls.chunk_work probes or four probe-set sizes (each unit rebuilds its probe table).
+          const unsigned long long rc = *(volatile unsigned long long*)&ctl->round_cost[par];
+          const int64_t target = max((int64_t)cls.chunk_work, (int64_t)(rc / (4ull * gridDim.x)));
+          for (uint32_t j0 = 0; j0 < nb; j0 += kPT) {
+            const uint32_t j = j0 + threadIdx.x;
+            uint32_t c = 0;
+            if (j < nb) {
+              if (kWing) {
+                const uint32_t x = W.fbig[par][j];
+                const uint32_t v = G.center_of[x], u = G.u_of[x];
+                const bool fv = cls.wing_from_v(G, v, u);
+                const int64_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
+                const int64_t d1 = fv ? G.offC[v + 1] - G.offC[v] : G.offK[u + 1] - G.offK[u];
+                const int64_t unit = max(target, 4 * psize);
+                int64_t k = ((int64_t)W.fchunks[par][j] + unit - 1) / unit;
+                k = min(k, min(d1, (int64_t)4096));
+                c = (uint32_t)max(k, (int64_t)1);
+              } else {
+                c = 1;
+              }
+              W.fchunks[par][j] = c;
+            }
+            uint32_t T;
+            const uint32_t incl = block_incl_scan(c, S.scan, T);
+            if (j < nb) W.uprefix[j] = carry + incl - c;
+            carry += T;
+          }
+          if (threadIdx.x == 0) {
+            W.uprefix[nb] = carry;
+            ctl->units = carry;
+            ctl->cur_big[par] = 0;
+          }
+        }
+        if (!grid_barrier(ctl)) return;
+        const unsigned nu = *(volatile unsigned*)&ctl->units;
+        while (true) {
+          if (threadIdx.x < 32) {  // warp 0: take a unit, find its item (last prefix <= u), 32-way
+            unsigned u = 0;
+            if (lane == 0) u = atomicAdd(&ctl->cur_big[par], 1u);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            uint32_t lo = 0, hi = nb;  // answer in [lo, hi)
+            if (u < nu) {
+              while (hi - lo > 1) {
+                const uint32_t step = (hi - lo + 31) / 32;
+                const uint32_t idx = lo + lane * step;
+                const bool le = idx < hi && W.uprefix[idx] <= u;
+                const unsigned bal = __ballot_sync(0xffffffffu, le);
+                const uint32_t last = 31 - __clz(bal);  // lane 0 always qualifies (prefix[lo] <= u)
+                lo = lo + last * step;
+                hi = min(lo + step, hi);
+              }
+            }
+            if (lane == 0) {
+              S.item = u;
+              S.hist[0] = lo;
+            }
+          }
+          __syncthreads();
+          const unsigned u = S.item, q = S.hist[0];
+          __syncthreads();
+          if (u >= nu) break;
+          const uint32_t x = W.fbig[par][q];
+          if (W.cnt[x] == 0) continue;  // uniform across the CTA
+          if (kWing) {
+            WingEdge E;
+            E.e1 = x;
+            E.v = G.center_of[x];
+            E.u = G.u_of[x];
+            E.from_v = cls.wing_from_v(G, E.v, E.u);
+            const uint32_t base = W.uprefix[q], nch = W.uprefix[q + 1] - base;
+            wing_item<LV_BLOCK>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work, u - base, nch);
+          } else {
+            tip_item_block(G, W, ctl, par, x, pool, S, work);
+          }
+        }
+      }
+      // Huge items, one at a time, each spread over every CTA of the grid.
+      const unsigned nh = *(volatile unsigned*)&ctl->flen_huge[par];
+      for (unsigned q = 0; q < nh; ++q) {
+        const uint32_t x = W.fhuge[par][q];
+        if (W.cnt[x] == 0) continue;  // frontier counts do not change during the phase
+        bool ok;
         if (kWing) {
           WingEdge E;
           E.e1 = x;
           E.v = G.center_of[x];
           E.u = G.u_of[x];
           E.from_v = cls.wing_from_v(G, E.v, E.u);
-          wing_item<true>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work);
+          ok = wing_item<LV_GRID>(G, W, ctl, par, E, nullptr, nullptr, 0, &S, work);
         } else {
-          tip_item_block(G, W, ctl, par, x, pool, S, work);
+          ok = tip_item_grid(G, W, ctl, par, x, S, work);
         }
+        if (!ok) return;
       }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 2);
     // ---- phase U: touched items move to bucket max(count, k) (all unpeeled items are above
     // k here); those entering the window join the near list and feed the next minimum.
     {
@@ -674,16 +988,22 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       if (lane == 0 && mn != kInf) atomicMin(&ctl->nm[npar], mn);
       const unsigned ns = *(volatile unsigned*)&ctl->flen_small[par];
       const unsigned nb = *(volatile unsigned*)&ctl->flen_big[par];
-      for (unsigned q = gtid; q < ns + nb; q += gthreads) {
-        const uint32_t x = q < ns ? W.fsmall[par][q] : W.fbig[par][q - ns];
+      const unsigned nh = *(volatile unsigned*)&ctl->flen_huge[par];
+      for (unsigned q = gtid; q < ns + nb + nh; q += gthreads) {
+        const uint32_t x = q < ns ? W.fsmall[par][q] : (q < ns + nb ? W.fbig[par][q - ns] : W.fhuge[par][q - ns - nb]);
         W.state[x] = PEELED;
       }
       if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->alive -= ns + nb;
+        ctl->alive -= ns + nb + nh;
         ctl->rounds += 1;
+        ctl->touched_total += nt;
+        ctl->n_small += ns;
+        ctl->n_big += nb;
+        ctl->n_huge += nh;
       }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 3);
   }
   unsigned long long w = work;
 #pragma unroll
@@ -857,7 +1177,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
 
   DevBuf<int64_t> cnt(N, s), wk, Sx;
   DevBuf<uint32_t> eti, iota, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
-  DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), tl0(N, s), tl1(N, s);
+  DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), fh0(N, s), fh1(N, s), tl0(N, s), tl1(N, s);
+  DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + 1, s);
+  DevBuf<uint32_t> gshared(std::max(G.nK, G.nC) + 1, s);
+  PB_CUDA_TRY(cudaMemsetAsync(gshared.get(), 0, gshared.bytes(), s));
   DevBuf<uint8_t> state(N, s), in_near(N, s);
   LiveSide liveK, liveC;
   liveK.n = G.nK;
@@ -931,6 +1254,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   W.fsmall[1] = fs1.get();
   W.fbig[0] = fb0.get();
   W.fbig[1] = fb1.get();
+  W.fchunks[0] = fc0.get();
+  W.fchunks[1] = fc1.get();
+  W.uprefix = upre.get();
+  W.fhuge[0] = fh0.get();
+  W.fhuge[1] = fh1.get();
+  W.gshared = gshared.get();
   W.tlist[0] = tl0.get();
   W.tlist[1] = tl1.get();
   W.gscratch = gscratch.get();
@@ -948,7 +1277,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
   DevBuf<Ctl> ctl(1, s);
   PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-  Classify cls{8192};
+  Classify cls{512, int64_t(1) << 40, 512};
+  // Thresholds may be lowered through the environment (tests use this to drive small graphs
+  // through the CTA- and grid-level paths).
+  if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);
+  if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
+  if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   Ctl* ctl_ptr = ctl.get();
   int launches = 0;
   while (true) {
@@ -983,6 +1317,15 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   }
   res.rounds = (int64_t)hctl.rounds;
   res.work = (int64_t)hctl.work;
+  if (const char* tr = getenv("PB_TRACE")) {
+    if (*tr && *tr != '0')
+      fprintf(stderr,
+              "[pb] peel %s: rounds %llu launches %d advances %llu | ms advance %.1f F %.1f P %.1f U %.1f | "
+              "near scanned %llu touched %llu items small %llu big %llu huge %llu work %llu\n",
+              kWing ? "wing" : "tip", hctl.rounds, launches, hctl.advances, hctl.phase_ns[0] / 1e6,
+              hctl.phase_ns[1] / 1e6, hctl.phase_ns[2] / 1e6, hctl.phase_ns[3] / 1e6, hctl.scanned,
+              hctl.touched_total, hctl.n_small, hctl.n_big, hctl.n_huge, hctl.work);
+  }
   return res;
 }
 

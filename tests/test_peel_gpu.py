@@ -100,3 +100,20 @@ def test_peel_inputs_on_device(ctx):
     pb.peel_e(dg, e_dev, out=out)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(out.cpu().numpy(), oracle.peel_edge(g, e)[0])
+
+
+@pytest.mark.parametrize("small,huge,chunk", [("0", "1000000000000", "8192"), ("0", "1000000000000", "1"),
+                                              ("0", "64", "8192"), ("8192", "200", "16")])
+def test_peel_levels_warp_cta_grid(ctx, monkeypatch, small, huge, chunk):
+    """Forces frontier items through the CTA-level (small=0), chunked (chunk=1: every item split
+    into as many work units as it has first-level entries) and grid-level (low huge) paths."""
+    monkeypatch.setenv("PB_PEEL_SMALL_WORK", small)
+    monkeypatch.setenv("PB_PEEL_HUGE_WORK", huge)
+    monkeypatch.setenv("PB_PEEL_CHUNK_WORK", chunk)
+    for g in [BipartiteGraph.zipf(500, 700, 6000, 1.3, 1201), BipartiteGraph.rmat(10, 9, 8000, 0.55, 0.15, 0.15, 0.15, 1202)]:
+        dg = ctx.upload(g)
+        for uv in (False, True):
+            e, _ = oracle.count(g, "EDGE", "ADEG", use_v=uv)
+            np.testing.assert_array_equal(pb.peel_e(dg, e, use_v=uv), oracle.peel_edge(g, e, use_v=uv)[0])
+            c, _ = oracle.count(g, "VERT", "ADEG", use_v=uv)
+            np.testing.assert_array_equal(pb.peel(dg, c, use_v=uv), oracle.peel_vert(g, c, use_v=uv)[0])
