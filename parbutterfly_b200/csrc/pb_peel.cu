@@ -60,6 +60,8 @@ struct Ctl {
   unsigned min_gain;          // pause for compaction once this many more items are peeled
   // Instrumentation (CTA 0): device time per phase and work counters.
   unsigned long long t_last, phase_ns[4];  // advance, F, P, U
+  unsigned long long barrier_timeout_ns;   // bound of every grid-barrier wait
+  unsigned test_skip_arrival;              // test hook: CTA 0 never arrives at grid barriers
   unsigned long long scanned, touched_total, n_small, n_big, n_huge, advances;
 };
 
@@ -125,7 +127,9 @@ __device__ bool grid_barrier(Ctl* ctl) {
     volatile unsigned* vgen = &ctl->bar_gen;
     const unsigned gen = *vgen;
     __threadfence();
-    const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
+    // (test hook) without CTA 0's arrival no CTA is last, so every wait runs out.
+    const unsigned arrived =
+        (blockIdx.x == 0 && *(volatile unsigned*)&ctl->test_skip_arrival) ? 0xFFFFFFFFu : atomicAdd(&ctl->bar_count, 1u);
     ok = 1;
     if (arrived == gridDim.x - 1) {
       atomicExch(&ctl->bar_count, 0u);
@@ -135,7 +139,7 @@ __device__ bool grid_barrier(Ctl* ctl) {
       const unsigned long long t0 = globaltimer_ns();
       while (*vgen == gen) {
         if (*(volatile unsigned*)&ctl->err) { ok = 0; break; }
-        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+        if (globaltimer_ns() - t0 > ctl->barrier_timeout_ns) {
           atomicOr(&ctl->err, ERR_TIMEOUT);
           ok = 0;
           break;
@@ -1275,6 +1279,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.alen[0] = (unsigned)N;
   hctl.alive_at_compact = (unsigned)N;
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
+  hctl.barrier_timeout_ns = kBarrierTimeoutNs;
+  if (const char* e = getenv("PB_PEEL_BARRIER_TIMEOUT_MS")) hctl.barrier_timeout_ns = 1000000ull * strtoull(e, nullptr, 10);
+  // Test hook: CTA 0 skips its arrivals, so the first grid barrier cannot complete and every
+  // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
+  if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
+    if (*e && *e != '0') hctl.test_skip_arrival = 1;
   DevBuf<Ctl> ctl(1, s);
   PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
   Classify cls{512, int64_t(1) << 40, 512};

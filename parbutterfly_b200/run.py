@@ -1,0 +1,62 @@
+"""Runs one named workload through the public API (used for profiling and ad-hoc timing).
+
+    python -m parbutterfly_b200.run count-edge --graph rmat20    # pb_count_edge(HASH, ACOCORE)
+    python -m parbutterfly_b200.run peel-edge --graph rmat15     # count, then pb_peel_edge
+    python -m parbutterfly_b200.run peel-vert --graph rmat20     # count, then pb_peel_vert
+
+Graphs: rmat20 = bipartite R-MAT 2^20 x 2^18, m = 2^24, (.55,.15,.15,.15), seed 2 (the
+benchmark workload); rmat15 = the same generator at 2^15 x 2^13, m = 2^19; rmat14 at
+2^14 x 2^12, m = 2^18; c1 = uniform 4096 x 4096, m = 131072, seed 1.
+"""
+import argparse
+import sys
+
+from . import butterflies as pb
+from .graph import BipartiteGraph, workload
+
+GRAPHS = {
+    "rmat20": lambda: BipartiteGraph.rmat(20, 18, 1 << 24, 0.55, 0.15, 0.15, 0.15, 2),
+    "rmat15": lambda: BipartiteGraph.rmat(15, 13, 1 << 19, 0.55, 0.15, 0.15, 0.15, 2),
+    "rmat14": lambda: BipartiteGraph.rmat(14, 12, 1 << 18, 0.55, 0.15, 0.15, 0.15, 2),
+    "c1": lambda: workload("c1"),
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["count-edge", "count-vert", "count-total", "peel-edge", "peel-vert"])
+    ap.add_argument("--graph", default="rmat15", choices=sorted(GRAPHS))
+    ap.add_argument("--count-type", default="HASH")
+    ap.add_argument("--rank-type", default="ACOCORE")
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args(argv)
+    g = GRAPHS[a.graph]()
+    with pb.Context(0) as ctx:
+        dg = ctx.upload(g)
+        for _ in range(a.repeat):
+            if a.case in ("count-edge", "peel-edge"):
+                e = pb.count_e(dg, a.count_type, a.rank_type)
+                s = ctx.stats()
+                print(f"count-edge w_rank={s['w_rank']} agg_ms={s['ms_agg_kernel']:.2f} total={int(e.sum()) // 4}")
+                if a.case == "peel-edge":
+                    pb.peel_e(dg, e)
+                    s = ctx.stats()
+                    print(f"peel-edge ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']}")
+            elif a.case in ("count-vert", "peel-vert"):
+                c = pb.count(dg, a.count_type, a.rank_type)
+                s = ctx.stats()
+                print(f"count-vert w_rank={s['w_rank']} agg_ms={s['ms_agg_kernel']:.2f} total={int(c.sum()) // 2}")
+                if a.case == "peel-vert":
+                    pb.peel(dg, c)
+                    s = ctx.stats()
+                    print(f"peel-vert ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']}")
+            else:
+                t = pb.count_total(dg, a.count_type, a.rank_type)
+                s = ctx.stats()
+                print(f"count-total w_rank={s['w_rank']} agg_ms={s['ms_agg_kernel']:.2f} total={t}")
+        dg.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

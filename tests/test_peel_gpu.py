@@ -117,3 +117,24 @@ def test_peel_levels_warp_cta_grid(ctx, monkeypatch, small, huge, chunk):
             np.testing.assert_array_equal(pb.peel_e(dg, e, use_v=uv), oracle.peel_edge(g, e, use_v=uv)[0])
             c, _ = oracle.count(g, "VERT", "ADEG", use_v=uv)
             np.testing.assert_array_equal(pb.peel(dg, c, use_v=uv), oracle.peel_vert(g, c, use_v=uv)[0])
+
+
+def test_barrier_timeout_reports_status_and_context_survives(ctx, monkeypatch):
+    """A grid-barrier wait that cannot complete (a phantom arrival, set by a test hook) runs out
+    after the configured bound; the call returns PB_ETIMEOUT and the context keeps working."""
+    import time
+    from parbutterfly_b200._ffi import PBError, PB_ETIMEOUT
+    g = BipartiteGraph.zipf(300, 400, 3000, 1.3, 1301)
+    dg = ctx.upload(g)
+    e = pb.count_e(dg)
+    monkeypatch.setenv("PB_PEEL_BARRIER_TIMEOUT_MS", "500")
+    monkeypatch.setenv("PB_PEEL_TEST_STUCK_BARRIER", "1")
+    t0 = time.time()
+    with pytest.raises(PBError) as ex:
+        pb.peel_e(dg, e)
+    assert ex.value.status == PB_ETIMEOUT
+    assert time.time() - t0 < 30
+    monkeypatch.delenv("PB_PEEL_TEST_STUCK_BARRIER")
+    monkeypatch.delenv("PB_PEEL_BARRIER_TIMEOUT_MS")
+    np.testing.assert_array_equal(pb.peel_e(dg, e), oracle.peel_edge(g, e)[0])
+    np.testing.assert_array_equal(pb.count_e(dg), e)
