@@ -218,6 +218,10 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
   CountResult cr = count_ranked(R, per, target, cfg, s);
   T.mark();
   tr.stage("count");
+  if (trace_on())
+    fprintf(stderr, "[pb] CTA modes (endpoints / wedges): dense %llu/%llu hash %llu/%llu global %llu/%llu hybrid %llu/%llu\n",
+            cr.mode_items[0], cr.mode_wedges[0], cr.mode_items[1], cr.mode_wedges[1], cr.mode_items[2],
+            cr.mode_wedges[2], cr.mode_items[3], cr.mode_wedges[3]);
   if (chk.get()) {
     uint32_t h[4];
     PB_CUDA_TRY(cudaMemcpyAsync(h, chk.get(), sizeof(h), cudaMemcpyDeviceToHost, s));

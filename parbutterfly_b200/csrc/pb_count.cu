@@ -21,6 +21,7 @@
 // of its prefix lengths, and lane/thread t locates its neighbour by a branchless binary search
 // over that scan, so consecutive threads read consecutive entries of N(v) (coalesced).
 #include <algorithm>
+#include <cstdlib>
 
 #include "pb_engine.cuh"
 #include "pb_prims.cuh"
@@ -47,6 +48,8 @@ struct Params {
   int64_t out_len;  // entries of out
   int64_t m2;       // slots of the ranked CSR
   uint32_t* err;    // record of the first bounds violation {code, index lo, index hi, aux}
+  uint32_t* out32;  // per-edge counts accumulated in 32 bits when every count fits (else null)
+  unsigned long long* mstats;  // per mode (dense, hash, hybrid, global): endpoints, wedges
 };
 
 // Records the first bounds violation (checked mode only).
@@ -62,7 +65,8 @@ __device__ __noinline__ void record_violation(uint32_t* err, uint32_t code, uint
 // (and reported as an error by the host) instead of being accessed.
 __device__ __forceinline__ void credit(const Params& P, uint64_t idx, int64_t v, uint32_t code) {
   if (idx >= (uint64_t)P.out_len) { record_violation(P.err, code, idx, 0); return; }
-  atomic_add_i64(&P.out[idx], v);
+  if (P.out32) atomicAdd(&P.out32[idx], (uint32_t)v);  // L2-resident 32-bit accumulation
+  else atomic_add_i64(&P.out[idx], v);
 }
 
 __device__ __forceinline__ bool slot_ok(const Params& P, uint64_t slot, uint32_t code) {
@@ -230,9 +234,11 @@ struct BlockShared {
   uint32_t incl[kBlock];
   uint32_t vs[kBlock];
   uint32_t vt[kBlock];
+  uint32_t len[kBlock];
   uint32_t scan[32];
   int64_t red[32];
   uint32_t item;
+  uint32_t cursor;
 };
 
 __device__ __forceinline__ uint32_t block_inclusive_scan_u32(uint32_t x, uint32_t* smem, uint32_t& total) {
@@ -265,10 +271,16 @@ __device__ __forceinline__ int64_t block_sum_i64(int64_t x, int64_t* smem) {
   return t;  // valid in thread 0
 }
 
-// Iterates every wedge of endpoint i with the whole CTA.
+// Iterates every wedge of endpoint i with the whole CTA.  Per chunk of kBlock neighbours, each
+// neighbour's prefix N(v)[0, L) is cut into pieces of at most kPiece wedges; warps claim pieces
+// from a shared-memory counter, locate a piece's neighbour once (binary search over the
+// chunk's inclusive piece counts) and walk it with 32 lanes, so consecutive lanes read
+// consecutive entries of N(v) and no per-wedge search is needed.
+constexpr uint32_t kPiece = 256;
+
 template <class F>
 __device__ __forceinline__ void block_wedges(uint32_t b, uint32_t e, const Params& P, BlockShared& S, F&& f) {
-  const uint32_t tid = threadIdx.x;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
   for (uint32_t j0 = b; j0 < e; j0 += kBlock) {
     const uint32_t j = j0 + tid;
     uint32_t L = 0, vt = 0, vs = 0;
@@ -279,33 +291,42 @@ __device__ __forceinline__ void block_wedges(uint32_t b, uint32_t e, const Param
       else { record_violation(P.err, 29, vt, j); L = 0; }
     }
     uint32_t T;
-    const uint32_t incl = block_inclusive_scan_u32(L, S.scan, T);
+    const uint32_t incl = block_inclusive_scan_u32((L + kPiece - 1) / kPiece, S.scan, T);
     S.incl[tid] = incl;
     S.vs[tid] = vs;
     S.vt[tid] = vt;
+    S.len[tid] = L;
+    if (tid == 0) S.cursor = 0;
     __syncthreads();
-    for (uint32_t t0 = 0; t0 < T; t0 += kBlock) {
-      const uint32_t t = t0 + tid;
-      if (t < T) {
-        uint32_t lo = 0;
+    while (true) {
+      uint32_t p = 0;
+      if (lane == 0) p = atomicAdd(&S.cursor, 1u);
+      p = __shfl_sync(0xffffffffu, p, 0);
+      if (p >= T) break;
+      uint32_t lo = 0;
 #pragma unroll
-        for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
-          if (S.incl[lo + step - 1] <= t) lo += step;
-        const uint32_t ex = lo ? S.incl[lo - 1] : 0u;
-        const uint32_t slot2 = S.vs[lo] + (t - ex);
-        if (slot_ok(P, slot2, 21)) f(j0 + lo, S.vt[lo], slot2, P.adj[slot2]);
+      for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+        if (S.incl[lo + step - 1] <= p) lo += step;
+      const uint32_t first_piece = lo ? S.incl[lo - 1] : 0u;
+      const uint32_t k0 = (p - first_piece) * kPiece;
+      const uint32_t kend = min(k0 + kPiece, S.len[lo]);
+      const uint32_t vsj = S.vs[lo], vtj = S.vt[lo];
+      for (uint32_t k = k0 + lane; k < kend; k += 32) {
+        const uint32_t slot2 = vsj + k;
+        if (slot_ok(P, slot2, 21)) f(j0 + lo, vtj, slot2, P.adj[slot2]);
       }
     }
     __syncthreads();
   }
 }
 
-enum Mode : uint32_t { MODE_DENSE = 0, MODE_HASH = 1, MODE_GLOBAL = 2 };
+enum Mode : uint32_t { MODE_DENSE = 0, MODE_HASH = 1, MODE_GLOBAL = 2, MODE_HYBRID = 3 };
 
 __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uint32_t* __restrict__ items,
                                                              const uint32_t* __restrict__ n_items_dev,
                                                              uint32_t* cursor, uint32_t* gscratch,
-                                                             uint32_t cap_dense, uint32_t cap_hash) {
+                                                             uint32_t cap_dense, uint32_t cap_hash,
+                                                             uint32_t hy_dense, uint32_t hy_hash) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BlockShared& S = *reinterpret_cast<BlockShared*>(smem_raw);
   uint32_t* table = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(BlockShared) + 15) & ~size_t(15)));
@@ -327,15 +348,47 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
     if (i <= cap_dense && (uint64_t)i <= 4ull * (uint64_t)W) mode = MODE_DENSE;
     else if ((uint64_t)2 * W <= cap_hash) mode = MODE_HASH;
     else if (i <= cap_dense) mode = MODE_DENSE;
-    else mode = MODE_GLOBAL;
+    else {
+      // Hybrid: dense counters for u2 < hy_dense (the low ranks, where R-MAT-like graphs put
+      // most wedge ends) plus a hash table for the rest, when the rest is small enough.  The
+      // number of wedges ending at or above hy_dense is exact: per neighbour, the prefix length
+      // minus the entries below hy_dense (one binary search each).
+      unsigned long long lo_w = 0;
+      for (uint32_t j = b + threadIdx.x; j < e; j += kBlock) {
+        const uint32_t v = P.adj[j] >> 1;
+        if (v >= P.n) continue;
+        const uint32_t vb = P.off[v];
+        const uint32_t below = lower_bound_u32(P.adj, vb, P.off[v + 1], hy_dense << 1) - vb;
+        lo_w += min(below, P.pref[j]);
+      }
+      const int64_t lo_total = block_sum_i64((int64_t)lo_w, S.red);
+      if (threadIdx.x == 0) S.item = (uint32_t)(W - lo_total > 0x7fffffff ? 0x7fffffff : W - lo_total);
+      __syncthreads();
+      const uint32_t hi_w = S.item;
+      __syncthreads();
+      mode = (2ull * hi_w <= hy_hash) ? MODE_HYBRID : MODE_GLOBAL;
+    }
+    if (threadIdx.x == 0 && P.mstats) {
+      atomicAdd(&P.mstats[mode], 1ull);
+      atomicAdd(&P.mstats[4 + mode], (unsigned long long)W);
+    }
     uint32_t tsize = 0, mask = 0;
     uint32_t* keys = table;
     uint32_t* vals = table + cap_hash;
+    if (mode == MODE_HYBRID) {
+      keys = table + hy_dense;
+      vals = keys + hy_hash;
+      tsize = hy_hash;
+      mask = tsize - 1;
+    }
     if (mode == MODE_DENSE) {
       for (uint32_t s = threadIdx.x; s < i; s += kBlock) table[s] = 0;
     } else if (mode == MODE_HASH) {
       tsize = max(64u, next_pow2(2u * (uint32_t)W));
       mask = tsize - 1;
+      for (uint32_t s = threadIdx.x; s < tsize; s += kBlock) { keys[s] = kEmpty; vals[s] = 0; }
+    } else if (mode == MODE_HYBRID) {
+      for (uint32_t s = threadIdx.x; s < hy_dense; s += kBlock) table[s] = 0;
       for (uint32_t s = threadIdx.x; s < tsize; s += kBlock) { keys[s] = kEmpty; vals[s] = 0; }
     }
     __syncthreads();
@@ -348,6 +401,12 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
     } else if (mode == MODE_HASH) {
       block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
         if (!table_insert(keys, vals, mask, u2t >> 1)) record_violation(P.err, 26, u2t >> 1, i);
+      });
+    } else if (mode == MODE_HYBRID) {
+      block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
+        const uint32_t u2 = u2t >> 1;
+        if (u2 < hy_dense) atomicAdd(&table[u2], 1u);
+        else if (!table_insert(keys, vals, mask, u2)) record_violation(P.err, 35, u2, i);
       });
     } else {
       block_wedges(b, e, P, S, [&](uint32_t, uint32_t, uint32_t, uint32_t u2t) {
@@ -365,6 +424,7 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
         if (u2 >= (mode == MODE_DENSE ? i : (uint32_t)P.n)) { record_violation(P.err, 24, u2, i); return; }
         if (mode == MODE_DENSE) w = table[u2];
         else if (mode == MODE_HASH) w = table_find(keys, vals, mask, u2);
+        else if (mode == MODE_HYBRID) w = u2 < hy_dense ? table[u2] : table_find(keys, vals, mask, u2);
         else w = gcnt[u2];
         if (w > 1) {
           if (P.per == EDGE) credit(P, P.eout[slot2], (int64_t)(w - 1), 13);
@@ -391,7 +451,17 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
             if (P.per == VERT) credit(P, s, bf, 16);
           }
         }
-      } else if (mode == MODE_HASH) {
+      } else if (mode == MODE_HASH || mode == MODE_HYBRID) {
+        if (mode == MODE_HYBRID) {
+          for (uint32_t s = threadIdx.x; s < hy_dense; s += kBlock) {
+            const int64_t w = table[s];
+            if (w >= 2) {
+              const int64_t bf = w * (w - 1) / 2;
+              mine += bf;
+              if (P.per == VERT) credit(P, s, bf, 36);
+            }
+          }
+        }
         for (uint32_t s = threadIdx.x; s < tsize; s += kBlock) {
           const uint32_t k = keys[s];
           if (k == kEmpty) continue;
@@ -428,6 +498,11 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
   }
 }
 
+__global__ void widen_u32_kernel(const uint32_t* __restrict__ in, int64_t n, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int64_t)in[i];
+}
+
 __global__ void classify_endpoints_kernel(const int64_t* __restrict__ wsum, int64_t n, int small_w, uint32_t cap_dense,
                                           uint32_t cap_hash, uint32_t* items, uint32_t* counts /* [0]=big [1]=global */) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -449,7 +524,7 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   if (out_len > 0) PB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int64_t) * out_len, s));
   if (n == 0 || R.w_rank == 0) return res;
   Params P{R.off.get(), R.adj.get(), R.pref.get(), per == EDGE ? R.eout.get() : nullptr, R.wsum.get(), n, per, out,
-           out_len, R.m2, nullptr};
+           out_len, R.m2, nullptr, nullptr, nullptr};
   DevBuf<uint32_t> err_local;
   if (cfg.err) {
     P.err = cfg.err;
@@ -458,17 +533,41 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     PB_CUDA_TRY(cudaMemsetAsync(err_local.get(), 0, 4 * sizeof(uint32_t), s));
     P.err = err_local.get();
   }
+  DevBuf<unsigned long long> mstats(8, s);
+  PB_CUDA_TRY(cudaMemsetAsync(mstats.get(), 0, 8 * sizeof(unsigned long long), s));
+  P.mstats = mstats.get();
+  // Per-edge counts fit 32 bits when (max degree - 1)^2 < 2^32: accumulate them in a 4-byte
+  // array (67 MB for 2^24 edges, L2-resident) and widen once at the end.
+  DevBuf<uint32_t> out32;
+  const uint64_t md = R.max_deg > 0 ? R.max_deg - 1 : 0;
+  const char* acc64 = getenv("PB_EDGE_ACC64");  // test hook: force 64-bit per-edge accumulation
+  const bool force64 = acc64 && *acc64 == '1';
+  if (per == EDGE && out_len > 0 && md * md < (1ull << 32) && !force64) {
+    out32.alloc(out_len, s);
+    PB_CUDA_TRY(cudaMemsetAsync(out32.get(), 0, out32.bytes(), s));
+    P.out32 = out32.get();
+  }
   const int sms = sm_count();
-  const int small_w = std::min(cfg.small_w, kWarpTable / 2);
+  int small_w = std::min(cfg.small_w, kWarpTable / 2);
+  int smem_bytes = cfg.smem_bytes;
+  // Test hooks: shrink the CTA table / the warp threshold so small graphs reach every CTA mode.
+  if (const char* ev = getenv("PB_COUNT_SMEM")) smem_bytes = std::max(16384, std::min(atoi(ev), cfg.smem_bytes));
+  if (const char* ev = getenv("PB_COUNT_SMALL_W")) small_w = std::max(0, std::min(atoi(ev), small_w));
+  int blocks_per_sm = cfg.blocks_per_sm;
+  if (const char* ev = getenv("PB_COUNT_BPS")) blocks_per_sm = std::max(1, std::min(atoi(ev), 4));
 
   // Block aggregator geometry.
   const size_t shared_fixed = (sizeof(BlockShared) + 15) & ~size_t(15);
-  const size_t table_bytes = (size_t)cfg.smem_bytes > shared_fixed ? (size_t)cfg.smem_bytes - shared_fixed : 0;
+  const size_t table_bytes = (size_t)smem_bytes > shared_fixed ? (size_t)smem_bytes - shared_fixed : 0;
   const uint32_t cap_dense = (uint32_t)(table_bytes / 4);
   uint32_t cap_hash = 1;
   while ((size_t)cap_hash * 2 * 8 <= table_bytes) cap_hash <<= 1;  // slots; keys + values
   if (cap_hash < 64) cap_hash = 64;
 
+  // Hybrid mode: half the table area as dense counters, the other half as a hash table.
+  const uint32_t hy_dense = (uint32_t)(table_bytes / 2 / 4);
+  uint32_t hy_hash = 1;
+  while ((size_t)hy_hash * 2 * 8 <= table_bytes / 2) hy_hash <<= 1;
   DevBuf<uint32_t> items(n, s), counts(3, s);
   PB_CUDA_TRY(cudaMemsetAsync(counts.get(), 0, 3 * sizeof(uint32_t), s));
   PB_LAUNCH(classify_endpoints_kernel, std::max(1, std::min(ceil_div(n, 256), sms * 8)), 256, 0, s, R.wsum.get(), n,
@@ -493,17 +592,24 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   }
   DevBuf<uint32_t> gscratch;
   if (hc[0] > 0) {
-    const int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * cfg.blocks_per_sm);
+    const int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * blocks_per_sm);
     if (hc[1] > 0) {
       gscratch.alloc((size_t)grid * (size_t)n, s);
       PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
     }
-    PB_CUDA_TRY(cudaFuncSetAttribute(count_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cfg.smem_bytes));
-    PB_LAUNCH(count_block_kernel, grid, kBlock, cfg.smem_bytes, s, P, items.get(), counts.get(), counts.get() + 2,
-              gscratch.get(), cap_dense, cap_hash);
+    PB_CUDA_TRY(cudaFuncSetAttribute(count_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+    PB_LAUNCH(count_block_kernel, grid, kBlock, smem_bytes, s, P, items.get(), counts.get(), counts.get() + 2,
+              gscratch.get(), cap_dense, cap_hash, hy_dense, hy_hash);
   }
+  if (P.out32)
+    PB_LAUNCH(widen_u32_kernel, std::max(1, std::min(ceil_div(out_len, 256), sms * 8)), 256, 0, s, P.out32, out_len, out);
   PB_CUDA_TRY(cudaEventRecord(e1, s));
   PB_CUDA_TRY(cudaEventSynchronize(e1));
+  {
+    unsigned long long h[8];
+    PB_CUDA_TRY(cudaMemcpy(h, P.mstats, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; ++k) { res.mode_items[k] = h[k]; res.mode_wedges[k] = h[4 + k]; }
+  }
   {
     uint32_t h[4];
     PB_CUDA_TRY(cudaMemcpy(h, P.err, sizeof(h), cudaMemcpyDeviceToHost));

@@ -52,8 +52,8 @@ struct CountConfig {
   int strategy = STRAT_AUTO;
   int small_w = 512;          // endpoints with W_i <= small_w go to the warp aggregator
   int block_threads = 512;    // threads of the block aggregator
-  int smem_bytes = 192 * 1024;  // dynamic shared memory of the block aggregator
-  int blocks_per_sm = 1;
+  int smem_bytes = 48 * 1024;   // dynamic shared memory of the block aggregator
+  int blocks_per_sm = 4;
   int split_w = 0;            // endpoints above this many wedges are split across CTAs (0: auto)
   uint32_t* err = nullptr;    // checked mode: device record of the first bounds violation
 };
@@ -66,6 +66,9 @@ void validate_ranked(const Ranked& R, int64_t m, uint32_t* err, cudaStream_t s);
 struct CountResult {
   int n_big = 0;
   double agg_ms = 0;
+  // CTA aggregator modes (dense, hash, global scratch, hybrid): endpoints and wedges.
+  unsigned long long mode_items[4] = {0, 0, 0, 0};
+  unsigned long long mode_wedges[4] = {0, 0, 0, 0};
 };
 CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConfig& cfg, cudaStream_t s);
 

@@ -143,3 +143,20 @@ def test_eti_matches_oracle(ctx, golden):
         dg = ctx.upload(g)
         for uv in (False, True):
             np.testing.assert_array_equal(pb.edge_to_idxs(dg, uv), oracle.edge_to_idxs(g, uv), err_msg=name)
+
+
+@pytest.mark.parametrize("smem,small_w,acc64", [("16384", "0", "0"), ("20000", "64", "1"), ("196608", "512", "1")])
+def test_cta_modes_vs_oracle(ctx, monkeypatch, smem, small_w, acc64):
+    """Small CTA tables push endpoints into the hash, hybrid and global-scratch modes; acc64
+    forces 64-bit per-edge accumulation (otherwise 32-bit when the degrees allow)."""
+    monkeypatch.setenv("PB_COUNT_SMEM", smem)
+    monkeypatch.setenv("PB_COUNT_SMALL_W", small_w)
+    monkeypatch.setenv("PB_EDGE_ACC64", acc64)
+    for g in [BipartiteGraph.rmat(14, 12, 150000, 0.55, 0.15, 0.15, 0.15, 41),
+              BipartiteGraph.powerlaw_u(3000, 20000, 200000, 2.0, 3000, 42)]:
+        dg = ctx.upload(g)
+        for rank in ["ADEG", "SIDE", "ACOCORE"]:
+            np.testing.assert_array_equal(pb.count(dg, "HASH", rank), oracle.count(g, "VERT", rank)[0])
+            np.testing.assert_array_equal(pb.count_e(dg, "HASH", rank), oracle.count(g, "EDGE", rank)[0])
+            assert pb.count_total(dg, "HASH", rank) == oracle.count(g, "TOTAL", rank)[0]
+        dg.close()
