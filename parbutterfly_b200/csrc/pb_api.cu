@@ -215,7 +215,9 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
     rc.alloc(R.n > 0 ? R.n : 1, s);
     target = rc.get();
   }
-  CountResult cr = count_ranked(R, per, target, cfg, s);
+  CountResult cr = cfg.strategy == STRAT_SORT   ? count_ranked_materialized(R, per, target, false, o.max_wedges, s)
+                   : cfg.strategy == STRAT_HIST ? count_ranked_materialized(R, per, target, true, o.max_wedges, s)
+                                                : count_ranked(R, per, target, cfg, s);
   T.mark();
   tr.stage("count");
   if (trace_on())

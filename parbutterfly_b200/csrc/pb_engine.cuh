@@ -71,6 +71,10 @@ struct CountResult {
   unsigned long long mode_wedges[4] = {0, 0, 0, 0};
 };
 CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConfig& cfg, cudaStream_t s);
+// SORT (hist = false) and HIST (hist = true) aggregators over materialised wedge batches of at
+// most max_wedges wedges (pb_agg_sort.cu).
+CountResult count_ranked_materialized(const Ranked& R, int per, int64_t* out, bool hist, int64_t max_wedges,
+                                      cudaStream_t s);
 
 // Peeling stage (pb_peel.cu).
 struct PeelResult {

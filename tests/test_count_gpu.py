@@ -160,3 +160,33 @@ def test_cta_modes_vs_oracle(ctx, monkeypatch, smem, small_w, acc64):
             np.testing.assert_array_equal(pb.count_e(dg, "HASH", rank), oracle.count(g, "EDGE", rank)[0])
             assert pb.count_total(dg, "HASH", rank) == oracle.count(g, "TOTAL", rank)[0]
         dg.close()
+
+
+@pytest.mark.parametrize("ct", ["SORT", "ASORT", "HIST", "AHIST"])
+@pytest.mark.parametrize("max_wedges", [2577500000, 5000])
+def test_materialized_aggregators_vs_oracle(ctx, ct, max_wedges):
+    """SORT (radix sort + runs) and HIST (semisort histogram) over wedge batches of at most
+    max_wedges wedges (-m); small -m forces many batches."""
+    for g in [BipartiteGraph.rmat(12, 11, 40000, 0.55, 0.15, 0.15, 0.15, 51),
+              BipartiteGraph.zipf(1500, 2500, 30000, 1.4, 52)]:
+        dg = ctx.upload(g)
+        for rank in ["ADEG", "SIDE", "COCORE"]:
+            np.testing.assert_array_equal(pb.count(dg, ct, rank, max_wedges=max_wedges), oracle.count(g, "VERT", rank)[0])
+            np.testing.assert_array_equal(pb.count_e(dg, ct, rank, max_wedges=max_wedges), oracle.count(g, "EDGE", rank)[0])
+            assert pb.count_total(dg, ct, rank, max_wedges=max_wedges) == oracle.count(g, "TOTAL", rank)[0]
+        dg.close()
+
+
+def test_hist_heavy_keys_overflow_path(ctx):
+    """A complete bipartite block makes a few (endpoint, u2) keys carry huge multiplicities and
+    fills semisort buckets with repeated keys; results must match the oracle."""
+    a, b = 40, 300
+    v = np.repeat(np.arange(a), b)
+    u = np.tile(np.arange(b), a)
+    extra_v = np.random.default_rng(3).integers(0, 400, 3000)
+    extra_u = np.random.default_rng(4).integers(0, 2000, 3000)
+    g = BipartiteGraph.from_edges(400, 2000, np.concatenate([v, extra_v]), np.concatenate([u, extra_u]))
+    dg = ctx.upload(g)
+    for ct in ["HIST", "SORT"]:
+        np.testing.assert_array_equal(pb.count(dg, ct, "ADEG"), oracle.count(g, "VERT", "ADEG")[0])
+        np.testing.assert_array_equal(pb.count_e(dg, ct, "DEG"), oracle.count(g, "EDGE", "DEG")[0])
