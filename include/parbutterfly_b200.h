@@ -153,6 +153,18 @@ pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, cons
 pb_status pb_peel_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* ecounts,
                        int64_t* wing);
 
+/* ---- many graphs at once --------------------------------------------------------------- */
+/* Count (butterfly_count.h:1634-1731) for k graphs in one pass: counts[g] receives nCount(g)
+ * per-vertex counts, each graph using its own count side as cmpWedgeCounts decides for it.
+ * The batch runs as one disjoint union on the device (one ranking, one aggregation, no
+ * per-graph launches); results equal k separate pb_count_vert calls. */
+pb_status pb_count_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts,
+                              int64_t* const* counts);
+/* Peel (butterfly_peel.h:896-934) for k graphs in one persistent launch: tips[g] receives the
+ * tip numbers of graph g from its per-vertex counts counts[g] (as from pb_count_vert_batch). */
+pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts,
+                             const int64_t* const* counts, int64_t* const* tips);
+
 /* ---- counting without device allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc where they need a
  * count (code running inside another framework's memory pool, paths that must not synchronise

@@ -25,6 +25,7 @@ EXPORTS = [
     "pb_count_total", "pb_peel_vert", "pb_peel_edge", "pb_csr_free", "pb_read_adjacency_hypergraph",
     "pb_write_adjacency_hypergraph", "pb_csr_validate", "pb_gen_uniform", "pb_gen_rmat",
     "pb_gen_powerlaw_u", "pb_gen_zipf", "pb_gen_batch_member", "pb_count_total_noalloc",
+    "pb_count_vert_batch", "pb_peel_vert_batch",
 ]
 
 
@@ -107,6 +108,8 @@ def lib():
         "pb_gen_zipf": (S, [I64, I64, I64, D, U64, C.POINTER(CSR)]),
         "pb_gen_batch_member": (S, [I32, C.POINTER(CSR)]),
         "pb_count_total_noalloc": (S, [C.POINTER(CSR), P, P, C.c_char_p, C.c_size_t]),
+        "pb_count_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
+        "pb_peel_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P), C.POINTER(P)]),
     }
     for name, (res, args) in sig.items():
         try:

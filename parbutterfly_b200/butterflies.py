@@ -211,3 +211,30 @@ def peel_e(dg: DeviceGraph, ecounts, peel_type="BATCHS", use_v=None, out=None, *
     o = make_opts(peel_type=peel_type, per="EDGE", use_v=use_v, **kw)
     dg.ctx.check(dg.ctx._lib.pb_peel_edge(dg.ctx.handle, dg.handle, C.byref(o), _ptr(c), _ptr(res)), "pb_peel_edge")
     return res[:dg.m] if out is None else res
+
+
+def count_batch(dgs, count_type="BATCHS", rank_type="ADEG", **kw):
+    """Per-vertex counts of several graphs in one pass (each with its own count side)."""
+    k = len(dgs)
+    sides = [(dg.nu if cmp_wedge_counts(dg)[0] else dg.nv) for dg in dgs]
+    outs = [np.zeros(max(n, 1), dtype=np.int64) for n in sides]
+    ctx = dgs[0].ctx
+    hs = (C.c_void_p * k)(*[dg.handle for dg in dgs])
+    ps = (C.c_void_p * k)(*[o.ctypes.data for o in outs])
+    o = make_opts(count_type, rank_type, per="VERT", **kw)
+    ctx.check(ctx._lib.pb_count_vert_batch(ctx.handle, hs, k, C.byref(o), ps), "pb_count_vert_batch")
+    return [out[:n] for out, n in zip(outs, sides)]
+
+
+def peel_batch(dgs, counts, peel_type="BATCHS", **kw):
+    """Tip numbers of several graphs in one persistent launch."""
+    k = len(dgs)
+    cs = [np.ascontiguousarray(c, dtype=np.int64) for c in counts]
+    tips = [np.zeros(max(c.size, 1), dtype=np.int64) for c in cs]
+    ctx = dgs[0].ctx
+    hs = (C.c_void_p * k)(*[dg.handle for dg in dgs])
+    pc = (C.c_void_p * k)(*[c.ctypes.data if c.size else None for c in cs])
+    pt = (C.c_void_p * k)(*[t.ctypes.data for t in tips])
+    o = make_opts(peel_type=peel_type, per="VERT", **kw)
+    ctx.check(ctx._lib.pb_peel_vert_batch(ctx.handle, hs, k, C.byref(o), pc, pt), "pb_peel_vert_batch")
+    return [t[:c.size] for t, c in zip(tips, cs)]

@@ -527,6 +527,58 @@ static pb_status peel_entry(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts,
   });
 }
 
+pb_status pb_count_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts,
+                              int64_t* const* counts) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(gs && counts && k > 0, PB_EINVAL, "null argument or empty batch");
+    pb_opts o = resolve_opts(opts);
+    o.use_v = 1;
+    cudaStream_t s = ctx->stream;
+    pb_graph U;
+    std::vector<int64_t> kbase, ksize;
+    build_union(gs, k, U, kbase, ksize, s);
+    DevBuf<int64_t> out(U.nu > 0 ? U.nu : 1, s);
+    run_count(ctx, &U, o, PB_VERT, 1, out.get());
+    for (int g = 0; g < k; ++g) {
+      PB_REQUIRE(counts[g] || ksize[g] == 0, PB_EINVAL, "null output in batch");
+      if (ksize[g])
+        PB_CUDA_TRY(cudaMemcpyAsync(counts[g], out.get() + kbase[g], sizeof(int64_t) * ksize[g], cudaMemcpyDefault, s));
+    }
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+  });
+}
+
+pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts,
+                             const int64_t* const* counts, int64_t* const* tips) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(gs && counts && tips && k > 0, PB_EINVAL, "null argument or empty batch");
+    resolve_opts(opts);
+    cudaStream_t s = ctx->stream;
+    pb_graph U;
+    std::vector<int64_t> kbase, ksize;
+    build_union(gs, k, U, kbase, ksize, s);
+    const int64_t n = U.nu;
+    if (n == 0) return;
+    DevBuf<int64_t> cin(n, s), tout(n, s);
+    for (int g = 0; g < k; ++g) {
+      PB_REQUIRE((counts[g] && tips[g]) || ksize[g] == 0, PB_EINVAL, "null buffer in batch");
+      if (ksize[g])
+        PB_CUDA_TRY(cudaMemcpyAsync(cin.get() + kbase[g], counts[g], sizeof(int64_t) * ksize[g], cudaMemcpyDefault, s));
+    }
+    Timer T(s);
+    T.mark();
+    PeelResult pr = peel_vertices(U, 1, cin.get(), tout.get(), s);
+    T.mark();
+    for (int g = 0; g < k; ++g)
+      if (ksize[g])
+        PB_CUDA_TRY(cudaMemcpyAsync(tips[g], tout.get() + kbase[g], sizeof(int64_t) * ksize[g], cudaMemcpyDefault, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    ctx->stats.ms_peel = T.ms(0, 1);
+    ctx->stats.peel_rounds = pr.rounds;
+    ctx->stats.peel_work = pr.work;
+  });
+}
+
 pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* counts, int64_t* tip) {
   return peel_entry(ctx, g, opts, counts, tip, false);
 }

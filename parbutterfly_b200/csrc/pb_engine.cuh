@@ -76,6 +76,11 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
 CountResult count_ranked_materialized(const Ranked& R, int per, int64_t* out, bool hist, int64_t max_wedges,
                                       cudaStream_t s);
 
+// Batches (pb_batch.cu): the disjoint union of k graphs, each graph's count side on the union's
+// U side (count with use_v = 1); kbase/ksize locate each graph's count side in the union.
+void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int64_t>& kbase,
+                 std::vector<int64_t>& ksize, cudaStream_t s);
+
 // Peeling stage (pb_peel.cu).
 struct PeelResult {
   int64_t rounds = 0;

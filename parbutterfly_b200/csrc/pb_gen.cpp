@@ -99,7 +99,7 @@ pb_status build_csr(int64_t nv, int64_t nu, std::vector<uint64_t>& keys, pb_csr_
 
 // Draws pairs from `draw` until m distinct ones exist, then builds the CSR.
 template <class Draw>
-pb_status draw_distinct(int64_t nv, int64_t nu, int64_t m, Draw draw, pb_csr_owned* out) {
+pb_status draw_distinct(int64_t nv, int64_t nu, int64_t m, Draw draw, pb_csr_owned* out, bool allow_short = false) {
   if (nv <= 0 || nu <= 0 || m < 0) return PB_EINVAL;
   if ((double)m > (double)nv * (double)nu) return PB_EINVAL;
   try {
@@ -110,7 +110,10 @@ pb_status draw_distinct(int64_t nv, int64_t nu, int64_t m, Draw draw, pb_csr_own
     const int64_t max_draws = 64 * m + 1000000;
     int64_t draws = 0;
     while ((int64_t)keys.size() < m) {
-      if (++draws > max_draws) return PB_EINVAL;
+      if (++draws > max_draws) {
+        if (allow_short) break;  // keep the distinct pairs drawn so far
+        return PB_EINVAL;
+      }
       uint64_t v, u;
       draw(v, u);
       uint64_t key = v * (uint64_t)nu + u;
@@ -201,7 +204,15 @@ pb_status pb_gen_rmat(int32_t log_nv, int32_t log_nu, int64_t m, double a, doubl
   }, out);
 }
 
+static pb_status gen_zipf_impl(int64_t nv, int64_t nu, int64_t m, double s, uint64_t seed, pb_csr_owned* out,
+                               bool allow_short);
+
 pb_status pb_gen_zipf(int64_t nv, int64_t nu, int64_t m, double s, uint64_t seed, pb_csr_owned* out) {
+  return gen_zipf_impl(nv, nu, m, s, seed, out, false);
+}
+
+static pb_status gen_zipf_impl(int64_t nv, int64_t nu, int64_t m, double s, uint64_t seed, pb_csr_owned* out,
+                               bool allow_short) {
   if (!out || nv <= 0 || nu <= 0) return PB_EINVAL;
   if (s <= 0) return pb_gen_uniform(nv, nu, m, seed, out);
   try {
@@ -216,7 +227,7 @@ pb_status pb_gen_zipf(int64_t nv, int64_t nu, int64_t m, double s, uint64_t seed
     return draw_distinct(nv, nu, m, [&](uint64_t& v, uint64_t& u) {
       v = pv[zv.sample(r)];
       u = pu[zu.sample(r)];
-    }, out);
+    }, out, allow_short);
   } catch (const std::bad_alloc&) {
     return PB_ENOMEM;
   }
@@ -303,10 +314,10 @@ pb_status pb_gen_batch_member(int32_t g, pb_csr_owned* out) {
   m = std::min<int64_t>(m, nu * nv);
   const bool zipf = (r.next() >> 63) != 0;
   uint64_t seed = r.next();
-  // A Zipf graph whose heavy ids saturate cannot reach m distinct pairs quickly; cap m at
-  // half the grid for those.
+  // A Zipf graph whose heavy ids saturate cannot reach m distinct pairs quickly: cap m at half
+  // the grid, and keep the distinct pairs drawn so far if 64 m + 10^6 draws do not reach it.
   if (zipf) m = std::min<int64_t>(m, nu * nv / 2);
-  return zipf ? pb_gen_zipf(nv, nu, m, 1.5, seed, out) : pb_gen_uniform(nv, nu, m, seed, out);
+  return zipf ? gen_zipf_impl(nv, nu, m, 1.5, seed, out, true) : pb_gen_uniform(nv, nu, m, seed, out);
 }
 
 }  // extern "C"
