@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 1
+#define PB_ABI_VERSION 2
 
 typedef enum {
   PB_OK = 0,
@@ -101,6 +101,14 @@ typedef struct {
   int64_t peel_rounds;    /* bucket rounds executed by the last peel call */
   int64_t peel_work;      /* wedges (tip) or intersection probes (wing) processed while peeling */
   double ms_agg_kernel;   /* device time of the aggregation kernels alone */
+  /* Learned scheduler (no counterpart in the reference): */
+  int32_t sched_used;     /* 1 when the learned scheduler made this call's choices, else 0 */
+  int32_t sched_choice;   /* peel calls: index of the work-unit setting that ran (0 = plain) */
+  int64_t sched_items;    /* count calls: block-aggregator items the scheduler decided */
+  double ms_sched;        /* scheduler time inside the call (features, inference, ordering) */
+  double sched_pred;      /* predicted time: SM cycles summed over items (count), ms (peel) */
+  double sched_meas;      /* measured time in the same unit */
+  double sched_mae_log2;  /* count calls: mean |log2(predicted / measured)| over the items */
 } pb_stats;
 
 typedef struct pb_ctx pb_ctx;
@@ -164,6 +172,53 @@ pb_status pb_count_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k,
  * tip numbers of graph g from its per-vertex counts counts[g] (as from pb_count_vert_batch). */
 pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts,
                              const int64_t* const* counts, int64_t* const* tips);
+
+/* ---- learned scheduler (no counterpart in the reference) -------------------------------- */
+/* The reference always runs the fixed strategy its flags name.  Here a cost model — a 3-layer
+ * MLP (16 -> 64 -> 64 -> 1, BF16 operands, FP32 accumulation, every product on the tensor
+ * cores) — predicts log2 of the time of each candidate choice and the call takes the least:
+ *   counting (opts.sched = PB_SCHED_LEARNED, HASH/BATCHS/BATCHWA/SERIAL count types): the
+ *     aggregation mode of every endpoint the block aggregator takes (dense window, shared hash
+ *     table, global scratch, hybrid), and the order endpoints are taken in (longest first);
+ *   peeling (opts.sched = PB_SCHED_LEARNED): the work-unit setting of the persistent peel kernel
+ *     (which items run on a warp, how a round's CTA work is cut into units, which items take the
+ *     whole grid) from a grid of PB_SCHED_PEEL_CANDIDATES settings (0 = the plain setting).
+ * Results are identical to the plain path's (every choice is exact).  Without an attached,
+ * trained model a LEARNED call runs the plain path (stats.sched_used = 0).
+ * The model learns from traces the plain path logs: with tracing on, every count call appends
+ * one row per block-aggregator item (12 features + one-hot mode, target log2 SM cycles) and
+ * every peel call one row (12 call features + 4 setting features, target log2 ms).  In explore
+ * mode the choices are drawn at random among the valid ones (seeded) so that the traces cover
+ * every choice. */
+#define PB_SCHED_FEATURES 16
+#define PB_SCHED_PEEL_CANDIDATES 54
+typedef enum { PB_SCHED_COUNT = 0, PB_SCHED_PEEL = 1 } pb_sched_target;
+typedef enum { PB_TRACE_OFF = 0, PB_TRACE_PLAIN = 1, PB_TRACE_EXPLORE = 2 } pb_trace_mode;
+typedef struct pb_sched_model pb_sched_model;
+/* A model with both cost models (count, peel) initialised from `seed`, on ctx's device. */
+pb_status pb_sched_model_create(pb_ctx* ctx, uint64_t seed, pb_sched_model** out);
+pb_status pb_sched_model_destroy(pb_sched_model* model);
+/* Trains one cost model on host rows X[n][PB_SCHED_FEATURES], targets y[n] (log2 time) with
+ * Adam for `epochs` passes of mini-batches of `batch` rows; *final_mse (may be NULL) receives the
+ * last epoch's mean squared error in standardised units. */
+pb_status pb_sched_train(pb_ctx* ctx, pb_sched_model* model, int32_t target, const float* X, const float* y, int64_t n,
+                         int32_t epochs, int32_t batch, float lr, float* final_mse);
+/* Predicted log2 time for host rows X[n][PB_SCHED_FEATURES] into y[n] (host). */
+pb_status pb_sched_predict(pb_ctx* ctx, pb_sched_model* model, int32_t target, const float* X, int64_t n, float* y);
+pb_status pb_sched_save(pb_ctx* ctx, const pb_sched_model* model, const char* path);
+pb_status pb_sched_load(pb_ctx* ctx, pb_sched_model* model, const char* path);
+/* Attaches a model to the context (NULL detaches); LEARNED calls on ctx use it. */
+pb_status pb_ctx_set_sched_model(pb_ctx* ctx, pb_sched_model* model);
+/* Trace logging on ctx: mode pb_trace_mode; seed drives explore-mode choices. */
+pb_status pb_trace_set(pb_ctx* ctx, int32_t mode, uint64_t seed);
+/* Number of rows logged for `target`; with X and y non-NULL copies up to cap rows out. */
+pb_status pb_trace_rows(pb_ctx* ctx, int32_t target, float* X, float* y, int64_t cap, int64_t* n);
+pb_status pb_trace_clear(pb_ctx* ctx);
+/* The tensor-core product the cost model runs on, exposed for testing: D[m][n] (FP32, row
+ * stride ldd) = sum_k A(m,k) B(n,k) with BF16 operands in device memory addressed by element
+ * strides, A(m,k) = A[m*sam + k*sak], B(n,k) = B[n*sbn + k*sbk]; 1 <= N <= 128. */
+pb_status pb_tc_gemm_bf16(pb_ctx* ctx, int64_t M, int32_t N, int64_t K, const void* A, int64_t sam, int64_t sak,
+                          const void* B, int64_t sbn, int64_t sbk, float* D, int64_t ldd);
 
 /* ---- counting without device allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc where they need a

@@ -25,8 +25,15 @@ EXPORTS = [
     "pb_count_total", "pb_peel_vert", "pb_peel_edge", "pb_csr_free", "pb_read_adjacency_hypergraph",
     "pb_write_adjacency_hypergraph", "pb_csr_validate", "pb_gen_uniform", "pb_gen_rmat",
     "pb_gen_powerlaw_u", "pb_gen_zipf", "pb_gen_batch_member", "pb_count_total_noalloc",
-    "pb_count_vert_batch", "pb_peel_vert_batch",
+    "pb_count_vert_batch", "pb_peel_vert_batch", "pb_sched_model_create", "pb_sched_model_destroy",
+    "pb_sched_train", "pb_sched_predict", "pb_sched_save", "pb_sched_load", "pb_ctx_set_sched_model",
+    "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16",
 ]
+
+SCHED_FEATURES = 16
+SCHED_PEEL_CANDIDATES = 54
+SCHED_COUNT, SCHED_PEEL = 0, 1
+TRACE_OFF, TRACE_PLAIN, TRACE_EXPLORE = 0, 1, 2
 
 
 class PBLibraryMissing(RuntimeError):
@@ -61,6 +68,9 @@ class Stats(C.Structure):
         ("ms_rank", C.c_double), ("ms_relabel", C.c_double), ("ms_scan", C.c_double),
         ("ms_count", C.c_double), ("ms_convert", C.c_double), ("ms_peel", C.c_double),
         ("peel_rounds", C.c_int64), ("peel_work", C.c_int64), ("ms_agg_kernel", C.c_double),
+        ("sched_used", C.c_int32), ("sched_choice", C.c_int32), ("sched_items", C.c_int64),
+        ("ms_sched", C.c_double), ("sched_pred", C.c_double), ("sched_meas", C.c_double),
+        ("sched_mae_log2", C.c_double),
     ]
 
 
@@ -110,6 +120,17 @@ def lib():
         "pb_count_total_noalloc": (S, [C.POINTER(CSR), P, P, C.c_char_p, C.c_size_t]),
         "pb_count_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
         "pb_peel_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P), C.POINTER(P)]),
+        "pb_sched_model_create": (S, [P, U64, C.POINTER(P)]),
+        "pb_sched_model_destroy": (S, [P]),
+        "pb_sched_train": (S, [P, P, I32, P, P, I64, I32, I32, C.c_float, C.POINTER(C.c_float)]),
+        "pb_sched_predict": (S, [P, P, I32, P, I64, P]),
+        "pb_sched_save": (S, [P, P, C.c_char_p]),
+        "pb_sched_load": (S, [P, P, C.c_char_p]),
+        "pb_ctx_set_sched_model": (S, [P, P]),
+        "pb_trace_set": (S, [P, I32, U64]),
+        "pb_trace_rows": (S, [P, I32, P, P, I64, C.POINTER(I64)]),
+        "pb_trace_clear": (S, [P]),
+        "pb_tc_gemm_bf16": (S, [P, I64, I32, I64, P, I64, I64, P, I64, I64, P, I64]),
     }
     for name, (res, args) in sig.items():
         try:

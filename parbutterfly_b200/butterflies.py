@@ -238,3 +238,95 @@ def peel_batch(dgs, counts, peel_type="BATCHS", **kw):
     o = make_opts(peel_type=peel_type, per="VERT", **kw)
     ctx.check(ctx._lib.pb_peel_vert_batch(ctx.handle, hs, k, C.byref(o), pc, pt), "pb_peel_vert_batch")
     return [t[:c.size] for t, c in zip(tips, cs)]
+
+
+class SchedModel:
+    """The learned scheduler's cost models (a pb_sched_model): one for the per-item aggregation
+    modes of counting, one for the work-unit setting of peeling."""
+
+    COUNT, PEEL = _ffi.SCHED_COUNT, _ffi.SCHED_PEEL
+
+    def __init__(self, ctx: Context, seed: int = 1):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        ctx.check(ctx._lib.pb_sched_model_create(ctx.handle, seed, C.byref(self._h)), "pb_sched_model_create")
+
+    def close(self):
+        if self._h:
+            self.ctx._lib.pb_sched_model_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def train(self, target: int, X, y, epochs=60, batch=1024, lr=3e-3) -> float:
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, _ffi.SCHED_FEATURES)
+        y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1)
+        assert X.shape[0] == y.shape[0]
+        mse = C.c_float()
+        self.ctx.check(self.ctx._lib.pb_sched_train(self.ctx.handle, self._h, target, X.ctypes.data, y.ctypes.data,
+                                                    X.shape[0], epochs, batch, lr, C.byref(mse)), "pb_sched_train")
+        return float(mse.value)
+
+    def predict(self, target: int, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, _ffi.SCHED_FEATURES)
+        y = np.zeros(X.shape[0], dtype=np.float32)
+        self.ctx.check(self.ctx._lib.pb_sched_predict(self.ctx.handle, self._h, target, X.ctypes.data, X.shape[0],
+                                                      y.ctypes.data), "pb_sched_predict")
+        return y
+
+    def save(self, path: str):
+        self.ctx.check(self.ctx._lib.pb_sched_save(self.ctx.handle, self._h, path.encode()), "pb_sched_save")
+
+    def load(self, path: str):
+        self.ctx.check(self.ctx._lib.pb_sched_load(self.ctx.handle, self._h, path.encode()), "pb_sched_load")
+
+    def attach(self):
+        """LEARNED calls on the model's context use this model from now on."""
+        self.ctx.check(self.ctx._lib.pb_ctx_set_sched_model(self.ctx.handle, self._h), "pb_ctx_set_sched_model")
+
+
+def detach_sched_model(ctx: Context):
+    ctx.check(ctx._lib.pb_ctx_set_sched_model(ctx.handle, None), "pb_ctx_set_sched_model")
+
+
+def trace_set(ctx: Context, mode: str = "plain", seed: int = 0):
+    """Trace logging of scheduler rows on ctx: mode "off", "plain" or "explore"."""
+    m = {"off": _ffi.TRACE_OFF, "plain": _ffi.TRACE_PLAIN, "explore": _ffi.TRACE_EXPLORE}[mode]
+    ctx.check(ctx._lib.pb_trace_set(ctx.handle, m, seed), "pb_trace_set")
+
+
+def trace_rows(ctx: Context, target: int):
+    """The rows logged for target (SchedModel.COUNT or .PEEL): X [n, 16] and y [n] (log2 time)."""
+    n = C.c_int64()
+    ctx.check(ctx._lib.pb_trace_rows(ctx.handle, target, None, None, 0, C.byref(n)), "pb_trace_rows")
+    X = np.zeros((n.value, _ffi.SCHED_FEATURES), dtype=np.float32)
+    y = np.zeros(n.value, dtype=np.float32)
+    if n.value:
+        ctx.check(ctx._lib.pb_trace_rows(ctx.handle, target, X.ctypes.data, y.ctypes.data, n.value, C.byref(n)),
+                  "pb_trace_rows")
+    return X, y
+
+
+def trace_clear(ctx: Context):
+    ctx.check(ctx._lib.pb_trace_clear(ctx.handle), "pb_trace_clear")
+
+
+def tc_gemm_bf16(ctx: Context, A, B):
+    """D = A @ B.T on the tensor cores for torch bf16 CUDA tensors A [M, K] and B [N, K]
+    (any strides); returns an fp32 [M, N] tensor."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    D = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    torch.cuda.synchronize()  # the context's stream is not ordered after torch's
+    ctx.check(ctx._lib.pb_tc_gemm_bf16(ctx.handle, M, N, K, A.data_ptr(), A.stride(0), A.stride(1), B.data_ptr(),
+                                       B.stride(0), B.stride(1), D.data_ptr(), N), "pb_tc_gemm_bf16")
+    return D

@@ -2,6 +2,7 @@
 // entry points (include/parbutterfly_b200.h).
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -10,7 +11,14 @@
 #include <vector>
 
 #include "pb_engine.cuh"
+#include "pb_mlp.cuh"
 #include "pb_prims.cuh"
+#include "pb_sched.cuh"
+
+struct pb_sched_model {
+  int device = 0;
+  pb::MlpModel count, peel;
+};
 
 struct pb_ctx {
   int device = 0;
@@ -19,6 +27,11 @@ struct pb_ctx {
   std::string last_error;
   pb_stats stats{};
   int64_t launches = 0;
+  // Learned scheduler: attached model and trace log (index: pb_sched_target).
+  pb_sched_model* model = nullptr;
+  int trace_mode = PB_TRACE_OFF;
+  uint64_t trace_seed = 0;
+  std::vector<float> trace_X[2], trace_y[2];
 };
 
 namespace pb {
@@ -202,6 +215,18 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
     case PB_HIST: case PB_AHIST: cfg.strategy = STRAT_HIST; break;
     default: cfg.strategy = STRAT_HASH; break;
   }
+  // Learned scheduler / trace hooks of the block aggregator (HASH and dense count types).
+  SchedHooks hooks;
+  const bool fused = cfg.strategy == STRAT_DENSE || cfg.strategy == STRAT_HASH;
+  if (fused && o.sched == PB_SCHED_LEARNED && ctx->model && ctx->model->count.trained)
+    hooks.model = &ctx->model->count;
+  if (fused && ctx->trace_mode != PB_TRACE_OFF) {
+    hooks.trace_X = &ctx->trace_X[PB_SCHED_COUNT];
+    hooks.trace_y = &ctx->trace_y[PB_SCHED_COUNT];
+    hooks.explore = ctx->trace_mode == PB_TRACE_EXPLORE && !hooks.model;
+    hooks.seed = ctx->trace_seed++;
+  }
+  if (hooks.model || hooks.trace_X) cfg.sched = &hooks;
   DevBuf<uint32_t> chk;
   if (check_mode()) {
     chk.alloc(4, s);
@@ -249,6 +274,52 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
   st.ms_count = T.ms(3, 4);
   st.ms_convert = T.ms(4, 5);
   st.ms_agg_kernel = cr.agg_ms;
+  st.sched_used = hooks.model ? 1 : 0;
+  st.sched_items = hooks.items;
+  st.ms_sched = hooks.ms;
+  st.sched_pred = hooks.pred_cycles;
+  st.sched_meas = hooks.meas_cycles;
+  st.sched_mae_log2 = hooks.mae_log2;
+}
+
+// Work-unit setting of one peel call: learned (when a trained model is attached and the call
+// asks for it), a random candidate (explore tracing) or the plain setting.  Fills the
+// scheduler fields of the stats; *row receives the call's cost-model row for the trace.
+PeelTuning peel_setting(pb_ctx* ctx, const pb_graph& g, int use_v, bool wing, const int64_t* cdev, const pb_opts& o,
+                        std::vector<float>& row, float* pred) {
+  pb_stats& st = ctx->stats;
+  st.sched_used = 0;
+  st.sched_choice = 0;
+  st.ms_sched = 0;
+  st.sched_pred = 0;
+  const bool learned = o.sched == PB_SCHED_LEARNED && ctx->model && ctx->model->peel.trained;
+  if (!learned && ctx->trace_mode == PB_TRACE_OFF) return PeelTuning();
+  auto t0 = std::chrono::steady_clock::now();
+  float f[kPeelCallFeatures];
+  peel_call_features(g, use_v, wing, cdev, f, ctx->stream);
+  int c = 0;
+  if (learned) {
+    c = choose_peel(ctx->model->peel, f, pred, ctx->stream);
+    st.sched_used = 1;
+    st.sched_pred = std::exp2((double)*pred);
+  } else if (ctx->trace_mode == PB_TRACE_EXPLORE) {
+    uint64_t z = (ctx->trace_seed++) * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    c = (int)((z ^ (z >> 31)) % (uint64_t)kPeelCandidates);
+  }
+  st.sched_choice = c;
+  row.assign(kMlpIn, 0.f);
+  peel_row(f, c, row.data());
+  st.ms_sched = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return peel_candidate(c);
+}
+
+void log_peel_trace(pb_ctx* ctx, const std::vector<float>& row, double ms) {
+  if (ctx->trace_mode == PB_TRACE_OFF || row.empty()) return;
+  auto& X = ctx->trace_X[PB_SCHED_PEEL];
+  X.insert(X.end(), row.begin(), row.end());
+  ctx->trace_y[PB_SCHED_PEEL].push_back((float)std::log2(std::max(ms, 1e-3)));
 }
 
 // Runs fn(out_dev) with a device buffer of len int64 and delivers it to a host or device
@@ -515,14 +586,19 @@ static pb_status peel_entry(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts,
       cdev = cin.get();
     }
     Timer T(s);
+    std::vector<float> row;
+    float pred = 0.f;
+    const PeelTuning tune = peel_setting(ctx, *g, use_v, edges, cdev, o, row, &pred);
     with_output(ctx, res, len, [&](int64_t* dev) {
       T.mark();
-      PeelResult pr = edges ? peel_edges(*g, use_v, cdev, dev, s) : peel_vertices(*g, use_v, cdev, dev, s);
+      PeelResult pr = edges ? peel_edges(*g, use_v, cdev, dev, s, tune) : peel_vertices(*g, use_v, cdev, dev, s, tune);
       T.mark();
       PB_CUDA_TRY(cudaStreamSynchronize(s));
       ctx->stats.ms_peel = T.ms(0, 1);
       ctx->stats.peel_rounds = pr.rounds;
       ctx->stats.peel_work = pr.work;
+      ctx->stats.sched_meas = ctx->stats.ms_peel;
+      log_peel_trace(ctx, row, ctx->stats.ms_peel);
     });
   });
 }
@@ -552,7 +628,7 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
                              const int64_t* const* counts, int64_t* const* tips) {
   return guarded(ctx, [&] {
     PB_REQUIRE(gs && counts && tips && k > 0, PB_EINVAL, "null argument or empty batch");
-    resolve_opts(opts);
+    const pb_opts o = resolve_opts(opts);
     cudaStream_t s = ctx->stream;
     pb_graph U;
     std::vector<int64_t> kbase, ksize;
@@ -566,8 +642,11 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
         PB_CUDA_TRY(cudaMemcpyAsync(cin.get() + kbase[g], counts[g], sizeof(int64_t) * ksize[g], cudaMemcpyDefault, s));
     }
     Timer T(s);
+    std::vector<float> row;
+    float pred = 0.f;
+    const PeelTuning tune = peel_setting(ctx, U, 1, false, cin.get(), o, row, &pred);
     T.mark();
-    PeelResult pr = peel_vertices(U, 1, cin.get(), tout.get(), s);
+    PeelResult pr = peel_vertices(U, 1, cin.get(), tout.get(), s, tune);
     T.mark();
     for (int g = 0; g < k; ++g)
       if (ksize[g])
@@ -576,6 +655,8 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
     ctx->stats.ms_peel = T.ms(0, 1);
     ctx->stats.peel_rounds = pr.rounds;
     ctx->stats.peel_work = pr.work;
+    ctx->stats.sched_meas = ctx->stats.ms_peel;
+    log_peel_trace(ctx, row, ctx->stats.ms_peel);
   });
 }
 
@@ -584,6 +665,166 @@ pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, cons
 }
 pb_status pb_peel_edge(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* ecounts, int64_t* wing) {
   return peel_entry(ctx, g, opts, ecounts, wing, true);
+}
+
+// ---- learned scheduler ---------------------------------------------------------------------
+static pb::MlpModel* model_of(pb_sched_model* m, int32_t target) {
+  PB_REQUIRE(m, PB_EINVAL, "null model");
+  PB_REQUIRE(target == PB_SCHED_COUNT || target == PB_SCHED_PEEL, PB_EINVAL, "target must be COUNT or PEEL");
+  return target == PB_SCHED_COUNT ? &m->count : &m->peel;
+}
+
+pb_status pb_sched_model_create(pb_ctx* ctx, uint64_t seed, pb_sched_model** out) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(out, PB_EINVAL, "null argument");
+    auto* m = new pb_sched_model();
+    try {
+      m->device = ctx->device;
+      m->count.init(seed, ctx->stream);
+      m->peel.init(seed ^ 0x5bd1e995ull, ctx->stream);
+      PB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    } catch (...) {
+      delete m;
+      throw;
+    }
+    *out = m;
+  });
+}
+
+pb_status pb_sched_model_destroy(pb_sched_model* model) {
+  if (!model) return PB_EINVAL;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(model->device);
+  cudaDeviceSynchronize();
+  delete model;
+  cudaSetDevice(prev);
+  return PB_OK;
+}
+
+pb_status pb_sched_train(pb_ctx* ctx, pb_sched_model* model, int32_t target, const float* X, const float* y, int64_t n,
+                         int32_t epochs, int32_t batch, float lr, float* final_mse) {
+  return guarded(ctx, [&] {
+    pb::MlpModel* m = model_of(model, target);
+    PB_REQUIRE(X && y && n > 0, PB_EINVAL, "empty training set");
+    PB_REQUIRE(model->device == ctx->device, PB_EINVAL, "model and context are on different devices");
+    m->s = ctx->stream;
+    const float mse = m->train(X, y, n, epochs, batch, lr, 0x2545F4914F6CDD1Dull ^ (uint64_t)n);
+    if (final_mse) *final_mse = mse;
+  });
+}
+
+pb_status pb_sched_predict(pb_ctx* ctx, pb_sched_model* model, int32_t target, const float* X, int64_t n, float* y) {
+  return guarded(ctx, [&] {
+    pb::MlpModel* m = model_of(model, target);
+    PB_REQUIRE(X && y, PB_EINVAL, "null argument");
+    if (n <= 0) return;
+    cudaStream_t s = ctx->stream;
+    DevBuf<float> Xd((size_t)n * pb::kMlpIn, s), yd(n, s);
+    PB_CUDA_TRY(cudaMemcpyAsync(Xd.get(), X, Xd.bytes(), cudaMemcpyHostToDevice, s));
+    m->predict_dev(Xd.get(), n, yd.get(), s);
+    PB_CUDA_TRY(cudaMemcpyAsync(y, yd.get(), yd.bytes(), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+  });
+}
+
+pb_status pb_sched_save(pb_ctx* ctx, const pb_sched_model* model, const char* path) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(model && path, PB_EINVAL, "null argument");
+    FILE* f = fopen(path, "wb");
+    PB_REQUIRE(f, PB_EIO, std::string("cannot write ") + path);
+    const char magic[8] = {'P', 'B', 'S', 'C', 'H', 'E', 'D', '1'};
+    bool ok = fwrite(magic, 1, 8, f) == 8;
+    for (const pb::MlpModel* m : {&model->count, &model->peel}) {
+      const std::vector<float> blob = m->pack();
+      const int32_t trained = m->trained ? 1 : 0;
+      const int64_t len = (int64_t)blob.size();
+      ok = ok && fwrite(&trained, 4, 1, f) == 1 && fwrite(&len, 8, 1, f) == 1 &&
+           fwrite(blob.data(), sizeof(float), blob.size(), f) == blob.size();
+    }
+    fclose(f);
+    PB_REQUIRE(ok, PB_EIO, std::string("short write to ") + path);
+  });
+}
+
+pb_status pb_sched_load(pb_ctx* ctx, pb_sched_model* model, const char* path) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(model && path, PB_EINVAL, "null argument");
+    FILE* f = fopen(path, "rb");
+    PB_REQUIRE(f, PB_EIO, std::string("cannot read ") + path);
+    char magic[8];
+    bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PBSCHED1", 8) == 0;
+    for (pb::MlpModel* m : {&model->count, &model->peel}) {
+      int32_t trained = 0;
+      int64_t len = 0;
+      ok = ok && fread(&trained, 4, 1, f) == 1 && fread(&len, 8, 1, f) == 1 && len == pb::mlp_param_count() + 34;
+      if (!ok) break;
+      std::vector<float> blob((size_t)len);
+      ok = fread(blob.data(), sizeof(float), blob.size(), f) == blob.size();
+      if (!ok) break;
+      m->unpack(blob, ctx->stream);
+      m->trained = trained != 0;
+    }
+    fclose(f);
+    PB_REQUIRE(ok, PB_EIO, std::string("not a scheduler model file: ") + path);
+  });
+}
+
+pb_status pb_ctx_set_sched_model(pb_ctx* ctx, pb_sched_model* model) {
+  if (!ctx) return PB_EINVAL;
+  if (model && model->device != ctx->device) return PB_EINVAL;
+  ctx->model = model;
+  return PB_OK;
+}
+
+pb_status pb_trace_set(pb_ctx* ctx, int32_t mode, uint64_t seed) {
+  if (!ctx) return PB_EINVAL;
+  if (mode < PB_TRACE_OFF || mode > PB_TRACE_EXPLORE) return PB_EINVAL;
+  ctx->trace_mode = mode;
+  ctx->trace_seed = seed;
+  return PB_OK;
+}
+
+pb_status pb_trace_rows(pb_ctx* ctx, int32_t target, float* X, float* y, int64_t cap, int64_t* n) {
+  if (!ctx || !n || (target != PB_SCHED_COUNT && target != PB_SCHED_PEEL)) return PB_EINVAL;
+  const int64_t rows = (int64_t)ctx->trace_y[target].size();
+  *n = rows;
+  if (X && y) {
+    const int64_t k = std::min(rows, cap);
+    std::memcpy(X, ctx->trace_X[target].data(), sizeof(float) * (size_t)k * pb::kMlpIn);
+    std::memcpy(y, ctx->trace_y[target].data(), sizeof(float) * (size_t)k);
+  }
+  return PB_OK;
+}
+
+pb_status pb_trace_clear(pb_ctx* ctx) {
+  if (!ctx) return PB_EINVAL;
+  for (int t = 0; t < 2; ++t) {
+    ctx->trace_X[t].clear();
+    ctx->trace_y[t].clear();
+  }
+  return PB_OK;
+}
+
+pb_status pb_tc_gemm_bf16(pb_ctx* ctx, int64_t M, int32_t N, int64_t K, const void* A, int64_t sam, int64_t sak,
+                          const void* B, int64_t sbn, int64_t sbk, float* D, int64_t ldd) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(A && B && D, PB_EINVAL, "null argument");
+    PB_REQUIRE(is_device_ptr(A) && is_device_ptr(B) && is_device_ptr(D), PB_EINVAL, "operands must be device memory");
+    cudaStream_t s = ctx->stream;
+    DevBuf<uint32_t> err(4, s);
+    PB_CUDA_TRY(cudaMemsetAsync(err.get(), 0, err.bytes(), s));
+    pb::GemmSpec g;
+    g.A = (const __nv_bfloat16*)A; g.sam = sam; g.sak = sak;
+    g.B = (const __nv_bfloat16*)B; g.sbn = sbn; g.sbk = sbk;
+    g.M = M; g.N = N; g.K = K;
+    g.epi = pb::GEMM_STORE; g.D = D; g.ldd = ldd;
+    pb::tc_gemm_bf16(g, err.get(), s);
+    uint32_t h = 0;
+    PB_CUDA_TRY(cudaMemcpyAsync(&h, err.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    PB_REQUIRE(h == 0, PB_ETIMEOUT, "tensor-core GEMM: bounded mbarrier wait ran out");
+  });
 }
 
 }  // extern "C"

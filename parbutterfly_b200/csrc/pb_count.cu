@@ -21,9 +21,12 @@
 // of its prefix lengths, and lane/thread t locates its neighbour by a branchless binary search
 // over that scan, so consecutive threads read consecutive entries of N(v) (coalesced).
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
+#include <vector>
 
 #include "pb_engine.cuh"
+#include "pb_mlp.cuh"
 #include "pb_prims.cuh"
 
 namespace pb {
@@ -50,6 +53,11 @@ struct Params {
   uint32_t* err;    // record of the first bounds violation {code, index lo, index hi, aux}
   uint32_t* out32;  // per-edge counts accumulated in 32 bits when every count fits (else null)
   unsigned long long* mstats;  // per mode (dense, hash, hybrid, global): endpoints, wedges
+  // Scheduler hooks of the block aggregator (all null on the plain path):
+  const uint8_t* modes;        // modes[q]: aggregation mode of item q chosen by the scheduler
+  const uint32_t* order;       // order[p]: item taken at position p of the work counter
+  uint8_t* mode_out;           // mode_out[q]: mode item q ran with
+  unsigned long long* cycles;  // cycles[q]: SM cycles item q took (clock64, thread 0)
 };
 
 // Records the first bounds violation (checked mode only).
@@ -336,16 +344,19 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
   while (true) {
     if (threadIdx.x == 0) S.item = atomicAdd(cursor, 1u);
     __syncthreads();
-    const uint32_t q = S.item;
+    const uint32_t qp = S.item;
     __syncthreads();
-    if (q >= n_items) break;
+    if (qp >= n_items) break;
+    const uint32_t q = P.order ? P.order[qp] : qp;
+    const long long t_item = clock64();
     const uint32_t i = items[q];
     const int64_t W = P.wsum[i + 1] - P.wsum[i];
     const uint32_t b = P.off[i], e = P.off[i + 1];
     const bool tag_i = !(P.adj[b] & 1u);
     const bool need_center = P.per == EDGE || (P.per == VERT && !tag_i);
     Mode mode;
-    if (i <= cap_dense && (uint64_t)i <= 4ull * (uint64_t)W) mode = MODE_DENSE;
+    if (P.modes) mode = (Mode)(P.modes[q] & 3u);
+    else if (i <= cap_dense && (uint64_t)i <= 4ull * (uint64_t)W) mode = MODE_DENSE;
     else if ((uint64_t)2 * W <= cap_hash) mode = MODE_HASH;
     else if (i <= cap_dense) mode = MODE_DENSE;
     else {
@@ -491,6 +502,10 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
       }
       __syncthreads();
     }
+    if (threadIdx.x == 0) {
+      if (P.mode_out) P.mode_out[q] = (uint8_t)mode;
+      if (P.cycles) P.cycles[q] = (unsigned long long)(clock64() - t_item);
+    }
   }
   if (P.per == TOTAL) {
     const int64_t s = block_sum_i64(total, S.red);
@@ -512,6 +527,114 @@ __global__ void classify_endpoints_kernel(const int64_t* __restrict__ wsum, int6
     const bool dense_ok = (uint64_t)i <= cap_dense;
     const bool hash_ok = (uint64_t)2 * W <= cap_hash;
     if (!dense_ok && !hash_ok) atomicAdd(&counts[1], 1u);
+  }
+}
+
+// ---- scheduler support ---------------------------------------------------------------------
+constexpr int kItemFeatures = 12;  // features per item; 4 one-hot mode slots follow
+
+// One warp per block-aggregator item: cost-model features and the valid modes (bit m set when
+// mode m can hold the item's multiplicity table; the global mode always can).
+__global__ void item_features_kernel(Params P, const uint32_t* __restrict__ items, uint32_t n_items,
+                                     uint32_t cap_dense, uint32_t cap_hash, uint32_t hy_dense, uint32_t hy_hash,
+                                     float* F, uint8_t* valid) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (int64_t q = warp; q < n_items; q += nwarps) {
+    const uint32_t i = items[q];
+    const int64_t W = P.wsum[i + 1] - P.wsum[i];
+    const uint32_t b = P.off[i], e = P.off[i + 1];
+    unsigned long long lo_w = 0, sumdeg = 0;
+    for (uint32_t j = b + lane; j < e; j += 32) {
+      const uint32_t v = P.adj[j] >> 1;
+      if (v >= P.n) continue;
+      const uint32_t vb = P.off[v], ve = P.off[v + 1];
+      sumdeg += ve - vb;
+      const uint32_t below = lower_bound_u32(P.adj, vb, ve, hy_dense << 1) - vb;
+      lo_w += min(below, P.pref[j]);
+    }
+    lo_w = warp_sum(lo_w);
+    sumdeg = warp_sum(sumdeg);
+    if (lane == 0) {
+      const int64_t hi = W - (int64_t)lo_w;
+      const uint64_t hi_c = hi > 0x7fffffff ? 0x7fffffffull : (uint64_t)(hi > 0 ? hi : 0);
+      const bool tag_i = !(P.adj[b] & 1u);
+      const bool need_center = P.per == EDGE || (P.per == VERT && !tag_i);
+      const uint32_t deg = e - b;
+      float* f = F + q * kMlpIn;
+      f[0] = log2f(1.f + (float)W);
+      f[1] = log2f(1.f + (float)i);
+      f[2] = log2f(1.f + (float)deg);
+      f[3] = log2f(1.f + (float)hi_c);
+      f[4] = log2f(1.f + (float)lo_w);
+      f[5] = log2f(1.f + (float)sumdeg);
+      f[6] = need_center ? 1.f : 0.f;
+      f[7] = P.per == EDGE ? 1.f : 0.f;
+      f[8] = log2f(1.f + (float)P.n);
+      f[9] = f[1] - f[0];
+      f[10] = P.out32 ? 1.f : 0.f;
+      f[11] = log2f(1.f + (float)W / (float)(deg ? deg : 1u));
+      for (int k = kItemFeatures; k < kMlpIn; ++k) f[k] = 0.f;
+      valid[q] = (uint8_t)((i <= cap_dense ? 1u : 0u) | ((uint64_t)2 * W <= cap_hash ? 2u : 0u) | 4u |
+                           (2ull * hi_c <= hy_hash ? 8u : 0u));
+    }
+  }
+}
+
+// Cost-model rows: item q with mode m is row 4q + m (features, then the one-hot of m).
+__global__ void sched_candidates_kernel(const float* __restrict__ F, uint32_t n_items, float* X) {
+  const int64_t total = (int64_t)n_items * 4 * kMlpIn;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / kMlpIn;
+    const int f = (int)(e - r * kMlpIn);
+    const int64_t q = r >> 2;
+    const int m = (int)(r & 3);
+    X[e] = f < kItemFeatures ? F[q * kMlpIn + f] : (f - kItemFeatures == m ? 1.f : 0.f);
+  }
+}
+
+// The valid mode with the least predicted log2 cycles; key orders items longest first.
+__global__ void sched_choose_kernel(const float* __restrict__ y, const uint8_t* __restrict__ valid, uint32_t n_items,
+                                    uint8_t* modes, float* pred, uint32_t* key, uint32_t* idx, uint32_t* n_global) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
+    int best = MODE_GLOBAL;
+    float by = y[q * 4 + MODE_GLOBAL];
+    for (int m = 0; m < 4; ++m) {
+      if (m == MODE_GLOBAL || !(valid[q] & (1u << m))) continue;
+      const float v = y[q * 4 + m];
+      if (v < by) { by = v; best = m; }
+    }
+    modes[q] = (uint8_t)best;
+    pred[q] = by;
+    const float c = fminf(fmaxf(by, 0.f), 63.f);
+    key[q] = 0xFFFFFFFFu - (uint32_t)(c * 67108864.f);  // descending predicted cycles
+    idx[q] = (uint32_t)q;
+    if (best == MODE_GLOBAL) atomicAdd(n_global, 1u);
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// A seeded random valid mode per item (exploration for trace collection).
+__global__ void sched_explore_kernel(const uint8_t* __restrict__ valid, uint32_t n_items, uint64_t seed,
+                                     uint8_t* modes, uint32_t* n_global) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t vm = valid[q];
+    const uint32_t c = __popc(vm);
+    uint32_t k = (uint32_t)(mix64(seed + 0x9E3779B97F4A7C15ull * (uint64_t)(q + 1)) % c);
+    int m = 0;
+    for (; m < 4; ++m)
+      if (vm & (1u << m)) {
+        if (k == 0) break;
+        --k;
+      }
+    modes[q] = (uint8_t)m;
+    if (m == MODE_GLOBAL) atomicAdd(n_global, 1u);
   }
 }
 
@@ -590,10 +713,67 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     }
     PB_LAUNCH(count_warp_kernel, sms * 3, kWarpsPerBlockSmall * 32, smem, s, P, small_w);
   }
+  // Scheduler: per-item modes (learned or exploring) and the record of what each item ran
+  // with and how long it took.
+  SchedHooks* sh = cfg.sched;
+  const bool sched_on = sh && hc[0] > 0 && (sh->model || sh->explore || sh->trace_X);
+  DevBuf<float> sF, sPred;
+  DevBuf<uint8_t> sValid, sModes, sUsed;
+  DevBuf<uint32_t> sOrder, sKey, sKeyAlt, sIdxAlt, sNG;
+  DevBuf<unsigned long long> sCyc;
+  bool need_global = hc[1] > 0;
+  if (sched_on) {
+    const uint32_t ni = hc[0];
+    cudaEvent_t a0, a1;
+    PB_CUDA_TRY(cudaEventCreate(&a0));
+    PB_CUDA_TRY(cudaEventCreate(&a1));
+    PB_CUDA_TRY(cudaEventRecord(a0, s));
+    sF.alloc((size_t)ni * kMlpIn, s);
+    sValid.alloc(ni, s);
+    sUsed.alloc(ni, s);
+    sCyc.alloc(ni, s);
+    sNG.alloc(1, s);
+    PB_CUDA_TRY(cudaMemsetAsync(sNG.get(), 0, sizeof(uint32_t), s));
+    PB_LAUNCH(item_features_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 32, 256), sms * 8)), 256, 0, s, P,
+              items.get(), ni, cap_dense, cap_hash, hy_dense, hy_hash, sF.get(), sValid.get());
+    const int g1 = std::max(1, std::min(ceil_div(ni, 256), sms * 8));
+    if (sh->model) {
+      DevBuf<float> X((size_t)ni * 4 * kMlpIn, s), y((size_t)ni * 4, s);
+      PB_LAUNCH(sched_candidates_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 4 * kMlpIn, 256), sms * 8)), 256,
+                0, s, sF.get(), ni, X.get());
+      sh->model->predict_dev(X.get(), (int64_t)ni * 4, y.get(), s);
+      sModes.alloc(ni, s);
+      sPred.alloc(ni, s);
+      sKey.alloc(ni, s);
+      sOrder.alloc(ni, s);
+      sKeyAlt.alloc(ni, s);
+      sIdxAlt.alloc(ni, s);
+      PB_LAUNCH(sched_choose_kernel, g1, 256, 0, s, y.get(), sValid.get(), ni, sModes.get(), sPred.get(), sKey.get(),
+                sOrder.get(), sNG.get());
+      const bool alt = radix_sort_pairs_u32(sKey.get(), sOrder.get(), sKeyAlt.get(), sIdxAlt.get(), ni, 0, 32, s);
+      P.order = alt ? sIdxAlt.get() : sOrder.get();
+    } else if (sh->explore) {
+      sModes.alloc(ni, s);
+      PB_LAUNCH(sched_explore_kernel, g1, 256, 0, s, sValid.get(), ni, sh->seed, sModes.get(), sNG.get());
+    }
+    P.modes = sModes.get();  // null when only the plain choices are traced
+    P.mode_out = sUsed.get();
+    P.cycles = sCyc.get();
+    uint32_t ng = 0;
+    PB_CUDA_TRY(cudaMemcpyAsync(&ng, sNG.get(), sizeof(ng), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaEventRecord(a1, s));
+    PB_CUDA_TRY(cudaEventSynchronize(a1));
+    if (P.modes) need_global = ng > 0;
+    float ms = 0;
+    PB_CUDA_TRY(cudaEventElapsedTime(&ms, a0, a1));
+    sh->ms = ms;
+    cudaEventDestroy(a0);
+    cudaEventDestroy(a1);
+  }
   DevBuf<uint32_t> gscratch;
   if (hc[0] > 0) {
     const int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * blocks_per_sm);
-    if (hc[1] > 0) {
+    if (need_global) {
       gscratch.alloc((size_t)grid * (size_t)n, s);
       PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
     }
@@ -616,6 +796,39 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     PB_REQUIRE(h[0] == 0, PB_ECUDA,
                "aggregation: bounds violation code " + std::to_string(h[0]) + " index " +
                    std::to_string(((uint64_t)h[2] << 32) | h[1]) + " aux " + std::to_string(h[3]));
+  }
+  if (sched_on) {
+    const uint32_t ni = hc[0];
+    std::vector<float> hF((size_t)ni * kMlpIn), hPred;
+    std::vector<uint8_t> hUsed(ni);
+    std::vector<unsigned long long> hCyc(ni);
+    PB_CUDA_TRY(cudaMemcpy(hF.data(), sF.get(), sF.bytes(), cudaMemcpyDeviceToHost));
+    PB_CUDA_TRY(cudaMemcpy(hUsed.data(), sUsed.get(), sUsed.bytes(), cudaMemcpyDeviceToHost));
+    PB_CUDA_TRY(cudaMemcpy(hCyc.data(), sCyc.get(), sCyc.bytes(), cudaMemcpyDeviceToHost));
+    if (sh->model) {
+      hPred.resize(ni);
+      PB_CUDA_TRY(cudaMemcpy(hPred.data(), sPred.get(), sPred.bytes(), cudaMemcpyDeviceToHost));
+    }
+    double pc = 0, mc = 0, mae = 0;
+    for (uint32_t q = 0; q < ni; ++q) {
+      const double cyc = (double)std::max<unsigned long long>(hCyc[q], 1ull);
+      const double lc = std::log2(cyc);
+      if (sh->trace_X) {
+        for (int f = 0; f < kMlpIn; ++f)
+          sh->trace_X->push_back(f < kItemFeatures ? hF[(size_t)q * kMlpIn + f]
+                                                   : (f - kItemFeatures == (int)hUsed[q] ? 1.f : 0.f));
+        sh->trace_y->push_back((float)lc);
+      }
+      mc += cyc;
+      if (sh->model) {
+        pc += std::exp2((double)hPred[q]);
+        mae += std::fabs((double)hPred[q] - lc);
+      }
+    }
+    sh->items = ni;
+    sh->meas_cycles = mc;
+    sh->pred_cycles = pc;
+    sh->mae_log2 = sh->model ? mae / ni : 0.0;
   }
   float ms = 0;
   PB_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));

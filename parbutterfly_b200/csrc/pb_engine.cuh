@@ -48,6 +48,21 @@ void edge_to_idxs(const pb_graph& g, int use_v, uint32_t* eti, cudaStream_t s);
 // Counting stage (pb_count.cu).  per: 0 VERT (out: rank-space counts [n]), 1 EDGE (out: [m]
 // in output edge order), 2 TOTAL (out: [1]).  `strategy` selects the aggregator.
 enum Strategy { STRAT_HASH = 0, STRAT_DENSE = 1, STRAT_SORT = 2, STRAT_HIST = 3, STRAT_AUTO = 4 };
+struct MlpModel;
+// Scheduler hooks of one counting call.  Each endpoint the block aggregator takes is one
+// scheduling item; its features (12 numbers) plus a one-hot of the aggregation mode (dense,
+// hash, global, hybrid) form one cost-model row, and the item's measured SM cycles its target.
+struct SchedHooks {
+  MlpModel* model = nullptr;  // learned: the mode with the least predicted cycles among the
+                              // valid ones, items taken longest-predicted first
+  bool explore = false;       // a seeded random valid mode per item (trace collection)
+  uint64_t seed = 0;
+  std::vector<float>* trace_X = nullptr;  // when set, rows are appended (16 floats per row)
+  std::vector<float>* trace_y = nullptr;  // with log2(cycles) targets
+  // Filled by the call.
+  int64_t items = 0;
+  double pred_cycles = 0, meas_cycles = 0, mae_log2 = 0, ms = 0;
+};
 struct CountConfig {
   int strategy = STRAT_AUTO;
   int small_w = 512;          // endpoints with W_i <= small_w go to the warp aggregator
@@ -56,6 +71,7 @@ struct CountConfig {
   int blocks_per_sm = 4;
   int split_w = 0;            // endpoints above this many wedges are split across CTAs (0: auto)
   uint32_t* err = nullptr;    // checked mode: device record of the first bounds violation
+  SchedHooks* sched = nullptr;
 };
 
 // Checked mode (PB_CHECK=1): kernels bounds-check indices read from memory and record the
@@ -86,7 +102,16 @@ struct PeelResult {
   int64_t rounds = 0;
   int64_t work = 0;
 };
-PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s);
-PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s);
+// Work-unit sizing of the persistent peel kernel (the defaults are the plain path's).
+struct PeelTuning {
+  int64_t small_work = 512;               // items up to this work run on one warp
+  int64_t huge_work = int64_t(1) << 40;   // items above this run on the whole grid
+  int64_t chunk_work = 512;               // minimum probes per CTA work unit (wing)
+  int64_t units_per_cta = 4;              // CTA work units per CTA and round (wing)
+};
+PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s,
+                         const PeelTuning& tune = PeelTuning());
+PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s,
+                      const PeelTuning& tune = PeelTuning());
 
 }  // namespace pb

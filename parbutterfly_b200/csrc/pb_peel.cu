@@ -638,6 +638,7 @@ struct Classify {
   int64_t small_work;
   int64_t huge_work;   // items above this run on the whole grid
   int64_t chunk_work;  // target probes per work unit of a CTA-level wing item
+  int64_t units_per_cta;  // work units per CTA a round's CTA-level wing work is cut into
 
   __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const {
     return G.wk[u] <= kWarpSlots / 2 && G.wk[u] <= small_work;
@@ -869,10 +870,12 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         // pulls units (item, slice) from a shared cursor.
         if (blockIdx.x == 0) {
           uint32_t carry = 0;
-          // Unit size: about four units per CTA over the round's CTA-level work, never below
-          // cls.chunk_work probes or four probe-set sizes (each unit rebuilds its probe table).
+          // Unit size: about cls.units_per_cta units per CTA over the round's CTA-level work,
+          // never below cls.chunk_work probes or four probe-set sizes (each unit rebuilds its
+          // probe table).
           const unsigned long long rc = *(volatile unsigned long long*)&ctl->round_cost[par];
-          const int64_t target = max((int64_t)cls.chunk_work, (int64_t)(rc / (4ull * gridDim.x)));
+          const int64_t target =
+              max((int64_t)cls.chunk_work, (int64_t)(rc / ((unsigned long long)cls.units_per_cta * gridDim.x)));
           for (uint32_t j0 = 0; j0 < nb; j0 += kPT) {
             const uint32_t j = j0 + threadIdx.x;
             uint32_t c = 0;
@@ -1162,7 +1165,8 @@ void compact_side(LiveSide& L, const uint32_t* off, const uint32_t* nbr, const u
 }
 
 template <bool kWing>
-PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t* out, cudaStream_t s) {
+PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t* out, cudaStream_t s,
+                    const PeelTuning& tune) {
   PeelResult res;
   Lists G{};
   const uint32_t* offK0 = use_v ? g.offU.get() : g.offV.get();
@@ -1287,7 +1291,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
   DevBuf<Ctl> ctl(1, s);
   PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-  Classify cls{512, int64_t(1) << 40, 512};
+  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
   if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);
@@ -1341,12 +1345,14 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
 
 }  // namespace
 
-PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s) {
-  return run_peel<false>(g, use_v, counts_dev, tip_dev, s);
+PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s,
+                         const PeelTuning& tune) {
+  return run_peel<false>(g, use_v, counts_dev, tip_dev, s, tune);
 }
 
-PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s) {
-  return run_peel<true>(g, use_v, ecounts_dev, wing_dev, s);
+PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s,
+                      const PeelTuning& tune) {
+  return run_peel<true>(g, use_v, ecounts_dev, wing_dev, s, tune);
 }
 
 }  // namespace pb

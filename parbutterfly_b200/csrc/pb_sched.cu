@@ -1,0 +1,114 @@
+// Learned scheduler, peeling side: the work-unit setting of a peel call (which items run on a
+// warp, how a round's CTA-level work is cut into units, which items take the whole grid) is
+// picked by the cost model from call-level features.  Candidates are a fixed grid of
+// PeelTuning values; candidate 0 is the plain path's setting.  The counting side (per-item
+// aggregation modes) lives with the aggregator in pb_count.cu.
+#include <cmath>
+#include <vector>
+
+#include "pb_engine.cuh"
+#include "pb_mlp.cuh"
+#include "pb_sched.cuh"
+
+namespace pb {
+
+namespace {
+
+__global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, unsigned long long* out) {
+  unsigned long long sum = 0, mx = 0, nz = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long v = c[i] > 0 ? (unsigned long long)c[i] : 0ull;
+    sum += v;
+    mx = v > mx ? v : mx;
+    nz += v ? 1ull : 0ull;
+  }
+  sum = warp_sum(sum);
+  nz = warp_sum(nz);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = y > mx ? y : mx;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&out[0], sum);
+    atomicMax(&out[1], mx);
+    atomicAdd(&out[2], nz);
+  }
+}
+
+constexpr int64_t kSmall[3] = {128, 256, 512};
+constexpr int64_t kUnits[3] = {2, 4, 8};
+constexpr int64_t kChunk[3] = {512, 256, 2048};
+constexpr int64_t kHuge[2] = {int64_t(1) << 40, int64_t(1) << 22};
+
+}  // namespace
+
+PeelTuning peel_candidate(int c) {
+  // c = ((small * 3 + units) * 3 + chunk) * 2 + huge, reordered so that c = 0 is the plain
+  // setting (small 512, units 4, chunk 512, huge never).
+  const int h = c % 2, ch = (c / 2) % 3, un = (c / 6) % 3, sm = (c / 18) % 3;
+  PeelTuning t;
+  t.small_work = kSmall[(sm + 2) % 3];
+  t.units_per_cta = kUnits[(un + 1) % 3];
+  t.chunk_work = kChunk[ch];
+  t.huge_work = kHuge[h];
+  return t;
+}
+
+void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* counts_dev, float* f, cudaStream_t s) {
+  const int64_t nK = use_v ? g.nu : g.nv, nC = use_v ? g.nv : g.nu;
+  const int64_t N = wing ? g.m : nK;
+  int uv = 0;
+  int64_t wmin = 0, wv = 0, wu = 0;
+  cmp_wedge_counts(g, &uv, &wmin, &wv, &wu, s);
+  unsigned long long h[3] = {0, 0, 0};
+  if (N > 0) {
+    DevBuf<unsigned long long> acc(3, s);
+    PB_CUDA_TRY(cudaMemsetAsync(acc.get(), 0, acc.bytes(), s));
+    PB_LAUNCH(count_stats_kernel, std::max(1, std::min(ceil_div(N, 256), sm_count() * 4)), 256, 0, s, counts_dev, N,
+              acc.get());
+    PB_CUDA_TRY(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  const double wK = use_v ? (double)wv : (double)wu;  // wedges centred on the other side's ids
+  const double wC = use_v ? (double)wu : (double)wv;
+  auto lg = [](double x) { return (float)std::log2(1.0 + (x > 0 ? x : 0)); };
+  f[0] = wing ? 1.f : 0.f;
+  f[1] = lg((double)N);
+  f[2] = lg((double)g.m);
+  f[3] = lg((double)nK);
+  f[4] = lg((double)nC);
+  f[5] = lg((double)g.max_deg);
+  f[6] = lg(wK);
+  f[7] = lg(wC);
+  f[8] = lg(nK ? (double)g.m / nK : 0.0);
+  f[9] = lg(nC ? (double)g.m / nC : 0.0);
+  f[10] = lg((double)h[1]);
+  f[11] = lg(h[2] ? (double)h[0] / (double)h[2] : 0.0);
+}
+
+void peel_row(const float* call_f, int c, float* row) {
+  const PeelTuning t = peel_candidate(c);
+  for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
+  row[12] = (float)std::log2((double)t.small_work);
+  row[13] = (float)std::log2((double)t.units_per_cta);
+  row[14] = (float)std::log2((double)t.chunk_work);
+  row[15] = t.huge_work < (int64_t(1) << 40) ? 1.f : 0.f;
+}
+
+int choose_peel(MlpModel& model, const float* call_f, float* pred_log2ms, cudaStream_t s) {
+  std::vector<float> X((size_t)kPeelCandidates * kMlpIn), y(kPeelCandidates);
+  for (int c = 0; c < kPeelCandidates; ++c) peel_row(call_f, c, X.data() + (size_t)c * kMlpIn);
+  DevBuf<float> Xd(X.size(), s), yd(kPeelCandidates, s);
+  PB_CUDA_TRY(cudaMemcpyAsync(Xd.get(), X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s));
+  model.predict_dev(Xd.get(), kPeelCandidates, yd.get(), s);
+  PB_CUDA_TRY(cudaMemcpyAsync(y.data(), yd.get(), sizeof(float) * kPeelCandidates, cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  int best = 0;
+  for (int c = 1; c < kPeelCandidates; ++c)
+    if (y[c] < y[best]) best = c;
+  if (pred_log2ms) *pred_log2ms = y[best];
+  return best;
+}
+
+}  // namespace pb

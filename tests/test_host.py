@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     L = _ffi.lib()
     missing = [s for s in decl if not hasattr(L, s)]
     assert missing == []
-    assert L.pb_abi_version() == 1
+    assert L.pb_abi_version() == 2
 
 
 def test_opts_defaults_match_reference_cli():
