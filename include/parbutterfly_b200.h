@@ -178,20 +178,24 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
  * MLP (16 -> 64 -> 64 -> 1, BF16 operands, FP32 accumulation, every product on the tensor
  * cores) — predicts log2 of the time of each candidate choice and the call takes the least:
  *   counting (opts.sched = PB_SCHED_LEARNED, HASH/BATCHS/BATCHWA/SERIAL count types): the
- *     aggregation mode of every endpoint the block aggregator takes (dense window, shared hash
- *     table, global scratch, hybrid), and the order endpoints are taken in (longest first);
+ *     aggregation mode of every endpoint the block aggregator takes, among the shared-memory
+ *     modes that can hold its table (dense window, hash table, dense window + hash table); the
+ *     global-scratch mode remains the fallback of endpoints none of them can hold;
  *   peeling (opts.sched = PB_SCHED_LEARNED): the work-unit setting of the persistent peel kernel
  *     (which items run on a warp, how a round's CTA work is cut into units, which items take the
- *     whole grid) from a grid of PB_SCHED_PEEL_CANDIDATES settings (0 = the plain setting).
+ *     whole grid) from a grid of PB_SCHED_WING_CANDIDATES (wing) or PB_SCHED_TIP_CANDIDATES
+ *     (tip) settings (0 = the plain setting).
  * Results are identical to the plain path's (every choice is exact).  Without an attached,
  * trained model a LEARNED call runs the plain path (stats.sched_used = 0).
  * The model learns from traces the plain path logs: with tracing on, every count call appends
  * one row per block-aggregator item (12 features + one-hot mode, target log2 SM cycles) and
  * every peel call one row (12 call features + 4 setting features, target log2 ms).  In explore
- * mode the choices are drawn at random among the valid ones (seeded) so that the traces cover
- * every choice. */
+ * mode count calls draw each item's mode at random among the valid ones (seeded) and peel calls
+ * sweep the setting grid cyclically (tip and wing calls each from setting seed mod
+ * the kind's number of candidates, one step per call), so that the traces cover every choice. */
 #define PB_SCHED_FEATURES 16
-#define PB_SCHED_PEEL_CANDIDATES 54
+#define PB_SCHED_WING_CANDIDATES 54
+#define PB_SCHED_TIP_CANDIDATES 21
 typedef enum { PB_SCHED_COUNT = 0, PB_SCHED_PEEL = 1 } pb_sched_target;
 typedef enum { PB_TRACE_OFF = 0, PB_TRACE_PLAIN = 1, PB_TRACE_EXPLORE = 2 } pb_trace_mode;
 typedef struct pb_sched_model pb_sched_model;

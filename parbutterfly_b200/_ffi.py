@@ -31,7 +31,8 @@ EXPORTS = [
 ]
 
 SCHED_FEATURES = 16
-SCHED_PEEL_CANDIDATES = 54
+SCHED_WING_CANDIDATES = 54
+SCHED_TIP_CANDIDATES = 21
 SCHED_COUNT, SCHED_PEEL = 0, 1
 TRACE_OFF, TRACE_PLAIN, TRACE_EXPLORE = 0, 1, 2
 

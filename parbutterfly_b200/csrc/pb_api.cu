@@ -31,6 +31,7 @@ struct pb_ctx {
   pb_sched_model* model = nullptr;
   int trace_mode = PB_TRACE_OFF;
   uint64_t trace_seed = 0;
+  uint64_t peel_sweep[2] = {0, 0};  // explore-mode position in the setting grid (tip, wing)
   std::vector<float> trace_X[2], trace_y[2];
 };
 
@@ -293,26 +294,23 @@ PeelTuning peel_setting(pb_ctx* ctx, const pb_graph& g, int use_v, bool wing, co
   st.ms_sched = 0;
   st.sched_pred = 0;
   const bool learned = o.sched == PB_SCHED_LEARNED && ctx->model && ctx->model->peel.trained;
-  if (!learned && ctx->trace_mode == PB_TRACE_OFF) return PeelTuning();
+  if (!learned && ctx->trace_mode == PB_TRACE_OFF) return plain_peel_tuning(wing);
   auto t0 = std::chrono::steady_clock::now();
   float f[kPeelCallFeatures];
   peel_call_features(g, use_v, wing, cdev, f, ctx->stream);
   int c = 0;
   if (learned) {
-    c = choose_peel(ctx->model->peel, f, pred, ctx->stream);
+    c = choose_peel(ctx->model->peel, f, wing, pred, ctx->stream);
     st.sched_used = 1;
     st.sched_pred = std::exp2((double)*pred);
   } else if (ctx->trace_mode == PB_TRACE_EXPLORE) {
-    uint64_t z = (ctx->trace_seed++) * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    c = (int)((z ^ (z >> 31)) % (uint64_t)kPeelCandidates);
+    c = (int)(ctx->peel_sweep[wing ? 1 : 0]++ % (uint64_t)peel_candidates(wing));  // a cyclic sweep
   }
   st.sched_choice = c;
   row.assign(kMlpIn, 0.f);
-  peel_row(f, c, row.data());
+  peel_row(f, wing, c, row.data());
   st.ms_sched = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  return peel_candidate(c);
+  return peel_candidate(wing, c);
 }
 
 void log_peel_trace(pb_ctx* ctx, const std::vector<float>& row, double ms) {
@@ -782,6 +780,7 @@ pb_status pb_trace_set(pb_ctx* ctx, int32_t mode, uint64_t seed) {
   if (mode < PB_TRACE_OFF || mode > PB_TRACE_EXPLORE) return PB_EINVAL;
   ctx->trace_mode = mode;
   ctx->trace_seed = seed;
+  ctx->peel_sweep[0] = ctx->peel_sweep[1] = seed;
   return PB_OK;
 }
 

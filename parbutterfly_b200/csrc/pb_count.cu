@@ -55,7 +55,6 @@ struct Params {
   unsigned long long* mstats;  // per mode (dense, hash, hybrid, global): endpoints, wedges
   // Scheduler hooks of the block aggregator (all null on the plain path):
   const uint8_t* modes;        // modes[q]: aggregation mode of item q chosen by the scheduler
-  const uint32_t* order;       // order[p]: item taken at position p of the work counter
   uint8_t* mode_out;           // mode_out[q]: mode item q ran with
   unsigned long long* cycles;  // cycles[q]: SM cycles item q took (clock64, thread 0)
 };
@@ -344,10 +343,9 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
   while (true) {
     if (threadIdx.x == 0) S.item = atomicAdd(cursor, 1u);
     __syncthreads();
-    const uint32_t qp = S.item;
+    const uint32_t q = S.item;
     __syncthreads();
-    if (qp >= n_items) break;
-    const uint32_t q = P.order ? P.order[qp] : qp;
+    if (q >= n_items) break;
     const long long t_item = clock64();
     const uint32_t i = items[q];
     const int64_t W = P.wsum[i + 1] - P.wsum[i];
@@ -582,34 +580,36 @@ __global__ void item_features_kernel(Params P, const uint32_t* __restrict__ item
   }
 }
 
-// Cost-model rows: item q with mode m is row 4q + m (features, then the one-hot of m).
+// Candidate modes of the learned choice: the shared-memory modes (the global-scratch mode is
+// the fallback of items no shared-memory mode can hold; it is never cheaper).
+__constant__ int kCandMode[3] = {MODE_DENSE, MODE_HASH, MODE_HYBRID};
+
+// Cost-model rows: item q with candidate c is row 3q + c (features, then the one-hot mode).
 __global__ void sched_candidates_kernel(const float* __restrict__ F, uint32_t n_items, float* X) {
-  const int64_t total = (int64_t)n_items * 4 * kMlpIn;
+  const int64_t total = (int64_t)n_items * 3 * kMlpIn;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = e / kMlpIn;
     const int f = (int)(e - r * kMlpIn);
-    const int64_t q = r >> 2;
-    const int m = (int)(r & 3);
+    const int64_t q = r / 3;
+    const int m = kCandMode[r - 3 * q];
     X[e] = f < kItemFeatures ? F[q * kMlpIn + f] : (f - kItemFeatures == m ? 1.f : 0.f);
   }
 }
 
-// The valid mode with the least predicted log2 cycles; key orders items longest first.
+// The valid shared-memory mode with the least predicted log2 cycles, else the global mode.
 __global__ void sched_choose_kernel(const float* __restrict__ y, const uint8_t* __restrict__ valid, uint32_t n_items,
-                                    uint8_t* modes, float* pred, uint32_t* key, uint32_t* idx, uint32_t* n_global) {
+                                    uint8_t* modes, float* pred, uint32_t* n_global) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
     int best = MODE_GLOBAL;
-    float by = y[q * 4 + MODE_GLOBAL];
-    for (int m = 0; m < 4; ++m) {
-      if (m == MODE_GLOBAL || !(valid[q] & (1u << m))) continue;
-      const float v = y[q * 4 + m];
+    float by = 1e30f;
+    for (int c = 0; c < 3; ++c) {
+      const int m = kCandMode[c];
+      if (!(valid[q] & (1u << m))) continue;
+      const float v = y[q * 3 + c];
       if (v < by) { by = v; best = m; }
     }
     modes[q] = (uint8_t)best;
-    pred[q] = by;
-    const float c = fminf(fmaxf(by, 0.f), 63.f);
-    key[q] = 0xFFFFFFFFu - (uint32_t)(c * 67108864.f);  // descending predicted cycles
-    idx[q] = (uint32_t)q;
+    pred[q] = best == MODE_GLOBAL ? -1.f : by;  // no prediction for the fallback
     if (best == MODE_GLOBAL) atomicAdd(n_global, 1u);
   }
 }
@@ -719,7 +719,7 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   const bool sched_on = sh && hc[0] > 0 && (sh->model || sh->explore || sh->trace_X);
   DevBuf<float> sF, sPred;
   DevBuf<uint8_t> sValid, sModes, sUsed;
-  DevBuf<uint32_t> sOrder, sKey, sKeyAlt, sIdxAlt, sNG;
+  DevBuf<uint32_t> sNG;
   DevBuf<unsigned long long> sCyc;
   bool need_global = hc[1] > 0;
   if (sched_on) {
@@ -738,20 +738,13 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
               items.get(), ni, cap_dense, cap_hash, hy_dense, hy_hash, sF.get(), sValid.get());
     const int g1 = std::max(1, std::min(ceil_div(ni, 256), sms * 8));
     if (sh->model) {
-      DevBuf<float> X((size_t)ni * 4 * kMlpIn, s), y((size_t)ni * 4, s);
-      PB_LAUNCH(sched_candidates_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 4 * kMlpIn, 256), sms * 8)), 256,
+      DevBuf<float> X((size_t)ni * 3 * kMlpIn, s), y((size_t)ni * 3, s);
+      PB_LAUNCH(sched_candidates_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 3 * kMlpIn, 256), sms * 8)), 256,
                 0, s, sF.get(), ni, X.get());
-      sh->model->predict_dev(X.get(), (int64_t)ni * 4, y.get(), s);
+      sh->model->predict_dev(X.get(), (int64_t)ni * 3, y.get(), s);
       sModes.alloc(ni, s);
       sPred.alloc(ni, s);
-      sKey.alloc(ni, s);
-      sOrder.alloc(ni, s);
-      sKeyAlt.alloc(ni, s);
-      sIdxAlt.alloc(ni, s);
-      PB_LAUNCH(sched_choose_kernel, g1, 256, 0, s, y.get(), sValid.get(), ni, sModes.get(), sPred.get(), sKey.get(),
-                sOrder.get(), sNG.get());
-      const bool alt = radix_sort_pairs_u32(sKey.get(), sOrder.get(), sKeyAlt.get(), sIdxAlt.get(), ni, 0, 32, s);
-      P.order = alt ? sIdxAlt.get() : sOrder.get();
+      PB_LAUNCH(sched_choose_kernel, g1, 256, 0, s, y.get(), sValid.get(), ni, sModes.get(), sPred.get(), sNG.get());
     } else if (sh->explore) {
       sModes.alloc(ni, s);
       PB_LAUNCH(sched_explore_kernel, g1, 256, 0, s, sValid.get(), ni, sh->seed, sModes.get(), sNG.get());
@@ -810,6 +803,7 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
       PB_CUDA_TRY(cudaMemcpy(hPred.data(), sPred.get(), sPred.bytes(), cudaMemcpyDeviceToHost));
     }
     double pc = 0, mc = 0, mae = 0;
+    int64_t npred = 0;
     for (uint32_t q = 0; q < ni; ++q) {
       const double cyc = (double)std::max<unsigned long long>(hCyc[q], 1ull);
       const double lc = std::log2(cyc);
@@ -819,16 +813,17 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
                                                    : (f - kItemFeatures == (int)hUsed[q] ? 1.f : 0.f));
         sh->trace_y->push_back((float)lc);
       }
-      mc += cyc;
-      if (sh->model) {
+      if (sh->model && hPred[q] >= 0.f) {  // items the model predicted (not the fallback)
+        mc += cyc;
         pc += std::exp2((double)hPred[q]);
         mae += std::fabs((double)hPred[q] - lc);
+        ++npred;
       }
     }
     sh->items = ni;
     sh->meas_cycles = mc;
     sh->pred_cycles = pc;
-    sh->mae_log2 = sh->model ? mae / ni : 0.0;
+    sh->mae_log2 = npred ? mae / npred : 0.0;
   }
   float ms = 0;
   PB_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));

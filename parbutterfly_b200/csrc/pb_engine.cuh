@@ -53,8 +53,8 @@ struct MlpModel;
 // scheduling item; its features (12 numbers) plus a one-hot of the aggregation mode (dense,
 // hash, global, hybrid) form one cost-model row, and the item's measured SM cycles its target.
 struct SchedHooks {
-  MlpModel* model = nullptr;  // learned: the mode with the least predicted cycles among the
-                              // valid ones, items taken longest-predicted first
+  MlpModel* model = nullptr;  // learned: the valid shared-memory mode with the least predicted
+                              // cycles (global scratch when none can hold the item)
   bool explore = false;       // a seeded random valid mode per item (trace collection)
   uint64_t seed = 0;
   std::vector<float>* trace_X = nullptr;  // when set, rows are appended (16 floats per row)
@@ -108,10 +108,19 @@ struct PeelTuning {
   int64_t huge_work = int64_t(1) << 40;   // items above this run on the whole grid
   int64_t chunk_work = 512;               // minimum probes per CTA work unit (wing)
   int64_t units_per_cta = 4;              // CTA work units per CTA and round (wing)
+  int64_t near_min = 32768;               // the near window holds at least this many items
+  int64_t near_div = 64;                  // ... or alive / near_div
 };
+// The plain path's settings: wing items never take the whole grid; tip items above 2^13
+// wedges do (one CTA per heavy vertex leaves the rest of the GPU idle in most rounds).
+inline PeelTuning plain_peel_tuning(bool wing) {
+  PeelTuning t;
+  if (!wing) t.huge_work = int64_t(1) << 13;
+  return t;
+}
 PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s,
-                         const PeelTuning& tune = PeelTuning());
+                         const PeelTuning& tune = plain_peel_tuning(false));
 PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s,
-                      const PeelTuning& tune = PeelTuning());
+                      const PeelTuning& tune = plain_peel_tuning(true));
 
 }  // namespace pb

@@ -63,6 +63,11 @@ struct Ctl {
   unsigned long long barrier_timeout_ns;   // bound of every grid-barrier wait
   unsigned test_skip_arrival;              // test hook: CTA 0 never arrives at grid barriers
   unsigned long long scanned, touched_total, n_small, n_big, n_huge, advances;
+  // Phase-P time of the rounds binned by log2 of their estimated work (frontier cost sum).
+  unsigned long long round_est[2];
+  unsigned long long pbin_ns[42], pbin_rounds[42], pbin_est[42];
+  // Near-window size: at least near_min items, or alive / near_div.
+  unsigned near_min, near_div;
 };
 
 
@@ -110,10 +115,19 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // CTA 0 charges the time since its previous mark to phase `ph` (called right after barriers).
-__device__ __forceinline__ void phase_mark(Ctl* ctl, int ph) {
+// Phase P is also binned by log2 of the round's estimated work (est).
+__device__ __forceinline__ void phase_mark(Ctl* ctl, int ph, unsigned long long est = 0) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const unsigned long long now = globaltimer_ns();
-    if (ctl->t_last) ctl->phase_ns[ph] += now - ctl->t_last;
+    if (ctl->t_last) {
+      ctl->phase_ns[ph] += now - ctl->t_last;
+      if (ph == 2) {
+        const int b = est ? min(41, 64 - __clzll(est)) : 0;
+        ctl->pbin_ns[b] += now - ctl->t_last;
+        ctl->pbin_rounds[b] += 1;
+        ctl->pbin_est[b] += est;
+      }
+    }
     ctl->t_last = now;
   }
 }
@@ -753,7 +767,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       if (threadIdx.x < 66 && S.hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], S.hist[threadIdx.x]);
       if (!grid_barrier(ctl)) return;
       // Every CTA derives the same bound: the smallest B with >= target items at distance < 2^B.
-      const unsigned target = max(32768u, alen2 / 64u);
+      const unsigned target = max(ctl->near_min, alen2 / max(1u, ctl->near_div));
       unsigned cum = 0;
       int B = 0;
       for (; B < 65; ++B) {
@@ -812,6 +826,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
             small = cls.tip_small(G, x);
             huge = !small && cls.tip_huge(G, x);
           }
+          atomicAdd(&ctl->round_est[par], (unsigned long long)(cost > 0 ? cost : 0));
           if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
           else if (huge) W.fhuge[par][atomicAdd(&ctl->flen_huge[par], 1u)] = x;
           else {
@@ -833,6 +848,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         ctl->flen_big[npar] = 0;
         ctl->flen_huge[npar] = 0;
         ctl->round_cost[npar] = 0;
+        ctl->round_est[npar] = 0;
         ctl->tlen[npar] = 0;
         ctl->cur_small[npar] = 0;
         ctl->cur_big[npar] = 0;
@@ -969,7 +985,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       }
     }
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 2);
+    phase_mark(ctl, 2, blockIdx.x == 0 && threadIdx.x == 0 ? *(volatile unsigned long long*)&ctl->round_est[par] : 0);
     // ---- phase U: touched items move to bucket max(count, k) (all unpeeled items are above
     // k here); those entering the window join the near list and feed the next minimum.
     {
@@ -1284,6 +1300,11 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.alive_at_compact = (unsigned)N;
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
   hctl.barrier_timeout_ns = kBarrierTimeoutNs;
+  hctl.near_min = (unsigned)tune.near_min;
+  hctl.near_div = (unsigned)tune.near_div;
+  // Diagnostic hooks for the window size.
+  if (const char* e = getenv("PB_PEEL_NEAR_MIN")) hctl.near_min = (unsigned)strtoul(e, nullptr, 10);
+  if (const char* e = getenv("PB_PEEL_NEAR_DIV")) hctl.near_div = (unsigned)strtoul(e, nullptr, 10);
   if (const char* e = getenv("PB_PEEL_BARRIER_TIMEOUT_MS")) hctl.barrier_timeout_ns = 1000000ull * strtoull(e, nullptr, 10);
   // Test hook: CTA 0 skips its arrivals, so the first grid barrier cannot complete and every
   // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
@@ -1339,6 +1360,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
               kWing ? "wing" : "tip", hctl.rounds, launches, hctl.advances, hctl.phase_ns[0] / 1e6,
               hctl.phase_ns[1] / 1e6, hctl.phase_ns[2] / 1e6, hctl.phase_ns[3] / 1e6, hctl.scanned,
               hctl.touched_total, hctl.n_small, hctl.n_big, hctl.n_huge, hctl.work);
+    if (*tr && *tr != '0')
+      for (int b = 0; b < 42; ++b)
+        if (hctl.pbin_rounds[b])
+          fprintf(stderr, "[pb]   P rounds with est work in [2^%d, 2^%d): %llu rounds, %.1f ms, est %.3g (%.3g/s)\n",
+                  b ? b - 1 : 0, b, hctl.pbin_rounds[b], hctl.pbin_ns[b] / 1e6, (double)hctl.pbin_est[b],
+                  hctl.pbin_ns[b] ? hctl.pbin_est[b] / (hctl.pbin_ns[b] / 1e9) : 0.0);
   }
   return res;
 }

@@ -1,8 +1,8 @@
 // Learned scheduler, peeling side: the work-unit setting of a peel call (which items run on a
 // warp, how a round's CTA-level work is cut into units, which items take the whole grid) is
 // picked by the cost model from call-level features.  Candidates are a fixed grid of
-// PeelTuning values; candidate 0 is the plain path's setting.  The counting side (per-item
-// aggregation modes) lives with the aggregator in pb_count.cu.
+// PeelTuning values per peel kind; candidate 0 is the plain path's setting.  The counting side
+// (per-item aggregation modes) lives with the aggregator in pb_count.cu.
 #include <cmath>
 #include <vector>
 
@@ -39,19 +39,30 @@ __global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, uns
 constexpr int64_t kSmall[3] = {128, 256, 512};
 constexpr int64_t kUnits[3] = {2, 4, 8};
 constexpr int64_t kChunk[3] = {512, 256, 2048};
-constexpr int64_t kHuge[2] = {int64_t(1) << 40, int64_t(1) << 22};
+constexpr int64_t kWingHuge[2] = {int64_t(1) << 40, int64_t(1) << 22};
+constexpr int64_t kTipHuge[7] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) << 12, int64_t(1) << 14,
+                                 int64_t(1) << 15, int64_t(1) << 16, int64_t(1) << 40};
 
 }  // namespace
 
-PeelTuning peel_candidate(int c) {
-  // c = ((small * 3 + units) * 3 + chunk) * 2 + huge, reordered so that c = 0 is the plain
-  // setting (small 512, units 4, chunk 512, huge never).
-  const int h = c % 2, ch = (c / 2) % 3, un = (c / 6) % 3, sm = (c / 18) % 3;
-  PeelTuning t;
-  t.small_work = kSmall[(sm + 2) % 3];
-  t.units_per_cta = kUnits[(un + 1) % 3];
-  t.chunk_work = kChunk[ch];
-  t.huge_work = kHuge[h];
+int peel_candidates(bool wing) { return wing ? kWingCandidates : kTipCandidates; }
+
+PeelTuning peel_candidate(bool wing, int c) {
+  PeelTuning t = plain_peel_tuning(wing);
+  if (wing) {
+    // c = ((small * 3 + units) * 3 + chunk) * 2 + huge, ordered so that c = 0 is the plain
+    // setting (small 512, units 4, chunk 512, huge never).
+    const int h = c % 2, ch = (c / 2) % 3, un = (c / 6) % 3, sm = (c / 18) % 3;
+    t.small_work = kSmall[(sm + 2) % 3];
+    t.units_per_cta = kUnits[(un + 1) % 3];
+    t.chunk_work = kChunk[ch];
+    t.huge_work = kWingHuge[h];
+  } else {
+    // c = small * 7 + huge; c = 0 is the plain setting (small 512, huge 2^13).
+    const int h = c % 7, sm = (c / 7) % 3;
+    t.small_work = kSmall[(sm + 2) % 3];
+    t.huge_work = kTipHuge[h];
+  }
   return t;
 }
 
@@ -87,25 +98,26 @@ void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* 
   f[11] = lg(h[2] ? (double)h[0] / (double)h[2] : 0.0);
 }
 
-void peel_row(const float* call_f, int c, float* row) {
-  const PeelTuning t = peel_candidate(c);
+void peel_row(const float* call_f, bool wing, int c, float* row) {
+  const PeelTuning t = peel_candidate(wing, c);
   for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
   row[12] = (float)std::log2((double)t.small_work);
   row[13] = (float)std::log2((double)t.units_per_cta);
   row[14] = (float)std::log2((double)t.chunk_work);
-  row[15] = t.huge_work < (int64_t(1) << 40) ? 1.f : 0.f;
+  row[15] = t.huge_work < (int64_t(1) << 40) ? (float)std::log2((double)t.huge_work) : 0.f;
 }
 
-int choose_peel(MlpModel& model, const float* call_f, float* pred_log2ms, cudaStream_t s) {
-  std::vector<float> X((size_t)kPeelCandidates * kMlpIn), y(kPeelCandidates);
-  for (int c = 0; c < kPeelCandidates; ++c) peel_row(call_f, c, X.data() + (size_t)c * kMlpIn);
-  DevBuf<float> Xd(X.size(), s), yd(kPeelCandidates, s);
+int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {
+  const int nc = peel_candidates(wing);
+  std::vector<float> X((size_t)nc * kMlpIn), y(nc);
+  for (int c = 0; c < nc; ++c) peel_row(call_f, wing, c, X.data() + (size_t)c * kMlpIn);
+  DevBuf<float> Xd(X.size(), s), yd(nc, s);
   PB_CUDA_TRY(cudaMemcpyAsync(Xd.get(), X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s));
-  model.predict_dev(Xd.get(), kPeelCandidates, yd.get(), s);
-  PB_CUDA_TRY(cudaMemcpyAsync(y.data(), yd.get(), sizeof(float) * kPeelCandidates, cudaMemcpyDeviceToHost, s));
+  model.predict_dev(Xd.get(), nc, yd.get(), s);
+  PB_CUDA_TRY(cudaMemcpyAsync(y.data(), yd.get(), sizeof(float) * nc, cudaMemcpyDeviceToHost, s));
   PB_CUDA_TRY(cudaStreamSynchronize(s));
   int best = 0;
-  for (int c = 1; c < kPeelCandidates; ++c)
+  for (int c = 1; c < nc; ++c)
     if (y[c] < y[best]) best = c;
   if (pred_log2ms) *pred_log2ms = y[best];
   return best;

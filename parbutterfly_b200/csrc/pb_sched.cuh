@@ -7,15 +7,17 @@
 namespace pb {
 
 constexpr int kPeelCallFeatures = 12;  // call-level features; 4 candidate slots follow
-constexpr int kPeelCandidates = 54;    // 3 small x 3 units x 3 chunk x 2 huge settings
+constexpr int kWingCandidates = 54;    // 3 small x 3 units x 3 chunk x 2 grid-level settings
+constexpr int kTipCandidates = 21;     // 3 small x 7 grid-level settings
 
-// Work-unit setting c of the candidate grid (c = 0: the plain path's setting).
-PeelTuning peel_candidate(int c);
+int peel_candidates(bool wing);
+// Work-unit setting c of the candidate grid of a peel kind (c = 0: the plain path's setting).
+PeelTuning peel_candidate(bool wing, int c);
 // Call-level features of a peel call (kPeelCallFeatures floats into f).
 void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* counts_dev, float* f, cudaStream_t s);
 // Cost-model row of candidate c for a call (kMlpIn floats).
-void peel_row(const float* call_f, int c, float* row);
+void peel_row(const float* call_f, bool wing, int c, float* row);
 // The candidate with the least predicted log2(ms); its prediction in *pred_log2ms.
-int choose_peel(MlpModel& model, const float* call_f, float* pred_log2ms, cudaStream_t s);
+int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s);
 
 }  // namespace pb

@@ -1,0 +1,109 @@
+"""Trains the learned scheduler's two cost models from traces the plain path logs.
+
+Traces come from seeded synthetic training graphs that are disjoint from the benchmark
+workloads (other seeds and sizes): bipartite R-MAT with three skews, Zipf-endpoint graphs and
+uniform graphs.  With tracing in explore mode the plain path logs
+  - count: one row per block-aggregator item of every count call (VERT and EDGE, HASH),
+    with a random valid aggregation mode per item (target log2 SM cycles of the item);
+  - peel:  one row per tip / wing peel call, sweeping the work-unit setting grid
+    (target log2 ms of the call).
+Both MLPs are then trained on the GPU (tensor-core forward / backward, Adam) and saved.
+
+    python -m parbutterfly_b200.sched_train --out sched.bin [--quick]
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+from . import butterflies as pb
+from .graph import BipartiteGraph
+
+# (kind, args, seed): seeds 7000+ are used by no benchmark workload.
+COUNT_GRAPHS = [
+    ("rmat", (17, 15, 1 << 21, 0.55, 0.15, 0.15, 0.15), 7001),
+    ("rmat", (18, 16, 1 << 22, 0.55, 0.15, 0.15, 0.15), 7002),
+    ("rmat", (18, 17, 1 << 22, 0.57, 0.19, 0.19, 0.05), 7003),
+    ("rmat", (16, 16, 1 << 21, 0.45, 0.25, 0.15, 0.15), 7004),
+    ("zipf", (1 << 16, 1 << 14, 1 << 20, 1.5), 7005),
+    ("zipf", (1 << 17, 1 << 15, 1 << 21, 1.2), 7006),
+    ("uniform", (1 << 14, 1 << 13, 1 << 20), 7007),
+]
+PEEL_GRAPHS = [
+    ("rmat", (15, 13, 1 << 18, 0.55, 0.15, 0.15, 0.15), 7101),
+    ("rmat", (16, 14, 1 << 19, 0.55, 0.15, 0.15, 0.15), 7102),
+    ("rmat", (16, 15, 1 << 19, 0.57, 0.19, 0.19, 0.05), 7103),
+    ("zipf", (1 << 15, 1 << 13, 1 << 18, 1.5), 7104),
+    ("uniform", (1 << 13, 1 << 12, 1 << 17), 7105),
+]
+
+
+def make(kind, args, seed) -> BipartiteGraph:
+    if kind == "rmat":
+        return BipartiteGraph.rmat(*args, seed)
+    if kind == "zipf":
+        return BipartiteGraph.zipf(*args, seed)
+    return BipartiteGraph.uniform(*args, seed)
+
+
+def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=54, log=print):
+    """Explore-mode traces: returns (Xc, yc, Xp, yp)."""
+    pb.trace_clear(ctx)
+    pb.trace_set(ctx, "explore", seed=1)
+    try:
+        for spec in count_graphs:
+            t0 = time.perf_counter()
+            dg = ctx.upload(make(*spec))
+            for rep in range(2):
+                pb.count(dg, "HASH", "ADEG")
+                pb.count_e(dg, "HASH", "ACOCORE")
+            dg.close()
+            log(f"[sched_train] count traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
+        for spec in peel_graphs:
+            t0 = time.perf_counter()
+            dg = ctx.upload(make(*spec))
+            c = pb.count(dg, "BATCHS", "ADEG")
+            ce = pb.count_e(dg, "BATCHS", "ADEG")
+            for k in range(peel_settings):
+                pb.peel(dg, c)
+                pb.peel_e(dg, ce)
+            dg.close()
+            log(f"[sched_train] peel traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
+    finally:
+        pb.trace_set(ctx, "off")
+    Xc, yc = pb.trace_rows(ctx, pb.SchedModel.COUNT)
+    Xp, yp = pb.trace_rows(ctx, pb.SchedModel.PEEL)
+    pb.trace_clear(ctx)
+    return Xc, yc, Xp, yp
+
+
+def train(ctx: pb.Context, Xc, yc, Xp, yp, seed=1, log=print) -> pb.SchedModel:
+    m = pb.SchedModel(ctx, seed=seed)
+    t0 = time.perf_counter()
+    mse_c = m.train(m.COUNT, Xc, yc, epochs=40, batch=1024, lr=3e-3)
+    mse_p = m.train(m.PEEL, Xp, yp, epochs=300, batch=64, lr=3e-3)
+    log(f"[sched_train] trained on {len(yc)} count rows (mse {mse_c:.3f}) and {len(yp)} peel rows "
+        f"(mse {mse_p:.3f}) in {time.perf_counter() - t0:.1f} s")
+    return m
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--quick", action="store_true", help="fewer graphs and peel settings")
+    a = ap.parse_args()
+    ctx = pb.Context(a.device)
+    cg, pg, ps = COUNT_GRAPHS, PEEL_GRAPHS, 54
+    if a.quick:
+        cg, pg, ps = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 18
+    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps)
+    m = train(ctx, Xc, yc, Xp, yp)
+    m.save(a.out)
+    print(f"[sched_train] saved {a.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -169,5 +169,7 @@ def test_peel_explore_every_setting_exact_and_learned(ctx):
         pb.peel_e(dg, ce, sched="learned")
         st = ctx.stats()
         assert st["sched_used"] == 1 and 0 <= st["sched_choice"] < 54 and st["sched_pred"] > 0
+        pb.peel(dg, c, sched="learned")
+        assert 0 <= ctx.stats()["sched_choice"] < 21
     finally:
         pb.detach_sched_model(ctx)
