@@ -6,9 +6,13 @@ One step = ACOCORE ranking + per-edge counting with HASH aggregation (-rankType 
 -per EDGE -countType HASH) + wing peeling (PBATCHS semantics) of the resulting counts.
 
 metric "wedges/s": W_rank (the wedges the ranked traversal enumerates, countWedgesScan) per
-second of a whole step (count + peel).  `value` runs on a device-resident graph with device
-outputs; `e2e` is the same step through the C ABI with pinned host buffers (graph upload,
-count download, count upload for peeling, wing download inside the timed region).
+second of a whole step (count + peel).  The step runs twice in the same process: with the plain
+fixed strategy and with the learned scheduler (opts.sched = LEARNED; cost models loaded from
+parbutterfly_b200/models/sched_b200.bin, trained on traces of other graphs); `value` is the
+learned step, `plain` the fixed-strategy step, and both must give identical counts and wing
+numbers.  `value` runs on a device-resident graph with device outputs; `e2e` is the learned step
+through the C ABI with pinned host buffers (graph upload, count download, count upload for
+peeling, wing download inside the timed region).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (torchrun): every rank runs an independent replica (the path does not shard on one
@@ -175,6 +179,23 @@ def reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+MODEL_PATH = os.path.join(ROOT, "parbutterfly_b200", "models", "sched_b200.bin")
+
+
+def load_or_train_model(ctx, pb):
+    """The learned scheduler's cost models: the committed B200-trained file, else a quick model
+    trained here on explore traces of the training graphs (never the benchmark graph)."""
+    m = pb.SchedModel(ctx, seed=1)
+    if os.path.exists(MODEL_PATH):
+        m.load(MODEL_PATH)
+        return m, {"source": os.path.relpath(MODEL_PATH, ROOT), "train_s": None}
+    from parbutterfly_b200 import sched_train as st
+    t0 = time.perf_counter()
+    Xc, yc, Xp, yp = st.collect(ctx, st.COUNT_GRAPHS[::2], st.PEEL_GRAPHS[:2], 21, log=lambda *a: None)
+    m = st.train(ctx, Xc, yc, Xp, yp, log=lambda *a: None)
+    return m, {"source": "trained at start-up (quick trace set)", "train_s": time.perf_counter() - t0}
+
+
 def our_arm(args, rank, world, local):
     import numpy as np
     import torch
@@ -186,49 +207,65 @@ def our_arm(args, rank, world, local):
     stream = torch.cuda.Stream(local)
     torch.cuda.set_stream(stream)
     ctx = pb.Context(local, stream=stream.cuda_stream)
+    model, model_info = load_or_train_model(ctx, pb)
+    model.attach()
     dg = ctx.upload(g)
     use_v, w_side = pb.cmp_wedge_counts(dg)
     ecount = torch.zeros(g.m, dtype=torch.int64, device="cuda")
     wing = torch.zeros(g.m, dtype=torch.int64, device="cuda")
+    ecount_p = torch.zeros(g.m, dtype=torch.int64, device="cuda")
+    wing_p = torch.zeros(g.m, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def step():
-        pb.count_e(dg, WORKLOAD["count_type"], WORKLOAD["rank_type"], use_v=use_v, out=ecount)
+    def step(sched, ec, wg):
+        pb.count_e(dg, WORKLOAD["count_type"], WORKLOAD["rank_type"], use_v=use_v, out=ec, sched=sched)
         s1 = ctx.stats()
-        pb.peel_e(dg, ecount, WORKLOAD["peel_type"], use_v=use_v, out=wing)
+        pb.peel_e(dg, ec, WORKLOAD["peel_type"], use_v=use_v, out=wg, sched=sched)
         s2 = ctx.stats()
         return s1, s2
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    barrier(world)
+    def timed(sched, ec, wg, clocks=None):
+        for _ in range(args.warmup):
+            step(sched, ec, wg)
+        torch.cuda.synchronize()
+        barrier(world)
+        if clocks:
+            clocks.start()
+        launches0 = ctx.kernel_launches()
+        durs, count_ms, peel_ms, agg_ms, stats = [], [], [], [], None
+        torch.cuda.synchronize()
+        barrier(world)
+        for _ in range(args.steps):
+            flush.fill_(1)  # evicts L2 (256 MiB > 126 MiB) outside the timed span
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s1, s2 = step(sched, ec, wg)
+            e1.record(stream)
+            e1.synchronize()
+            durs.append(e0.elapsed_time(e1))
+            count_ms.append(sum(s1[k] for k in ("ms_rank", "ms_relabel", "ms_scan", "ms_count", "ms_convert")))
+            agg_ms.append(s1["ms_agg_kernel"])
+            peel_ms.append(s2["ms_peel"])
+            stats = (s1, s2)
+        torch.cuda.synchronize()
+        barrier(world)
+        launches = ctx.kernel_launches() - launches0
+        clk = clocks.stop() if clocks else None
+        ms_step = max_over_ranks(sum(durs) / len(durs), world)
+        return {"ms_step": ms_step, "count_ms": statistics.mean(count_ms), "peel_ms": statistics.mean(peel_ms),
+                "agg_ms": statistics.mean(agg_ms), "stats": stats, "launches": launches, "clocks": clk}
+
     clocks = ClockSampler(local)
-    clocks.start()
-    launches0 = ctx.kernel_launches()
-    durs, count_ms, peel_ms, agg_ms, stats = [], [], [], [], None
-    torch.cuda.synchronize()
-    barrier(world)
-    for _ in range(args.steps):
-        flush.fill_(1)  # evicts L2 (256 MiB > 126 MiB) outside the timed span
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s1, s2 = step()
-        e1.record(stream)
-        e1.synchronize()
-        durs.append(e0.elapsed_time(e1))
-        count_ms.append(sum(s1[k] for k in ("ms_rank", "ms_relabel", "ms_scan", "ms_count", "ms_convert")))
-        agg_ms.append(s1["ms_agg_kernel"])
-        peel_ms.append(s2["ms_peel"])
-        stats = (s1, s2)
-    torch.cuda.synchronize()
-    barrier(world)
-    launches = ctx.kernel_launches() - launches0
-    clk = clocks.stop()
-    ms_step = max_over_ranks(sum(durs) / len(durs), world)
-    s1, s2 = stats
+    plain = timed("plain", ecount_p, wing_p)
+    learned = timed("learned", ecount, wing, clocks)
+    assert torch.equal(ecount, ecount_p) and torch.equal(wing, wing_p), "learned and plain results differ"
+    s1, s2 = learned["stats"]
+    ms_step = learned["ms_step"]
+    count_ms, peel_ms, agg_ms = learned["count_ms"], learned["peel_ms"], learned["agg_ms"]
+    launches, clk = learned["launches"], learned["clocks"]
     w_rank = int(s1["w_rank"])
     value = w_rank * world / (ms_step / 1e3)
+    plain_value = w_rank * world / (plain["ms_step"] / 1e3)
 
     # ---- end to end through the C ABI with pinned host buffers ------------------------------------
     host = {name: torch.from_numpy(getattr(g, name)).pin_memory() for name in ("offsetsV", "edgesV", "offsetsU", "edgesU")}
@@ -242,9 +279,9 @@ def our_arm(args, rank, world, local):
                      host["offsetsU"].data_ptr(), host["edgesU"].data_ptr())
         h = C.c_void_p()
         ctx.check(ctx._lib.pb_graph_upload(ctx.handle, C.byref(s), C.byref(h)), "pb_graph_upload")
-        o = pb.make_opts(WORKLOAD["count_type"], WORKLOAD["rank_type"], per="EDGE", use_v=use_v)
+        o = pb.make_opts(WORKLOAD["count_type"], WORKLOAD["rank_type"], per="EDGE", use_v=use_v, sched="learned")
         ctx.check(ctx._lib.pb_count_edge(ctx.handle, h, C.byref(o), ec_host.data_ptr()), "pb_count_edge")
-        o2 = pb.make_opts(peel_type=WORKLOAD["peel_type"], per="EDGE", use_v=use_v)
+        o2 = pb.make_opts(peel_type=WORKLOAD["peel_type"], per="EDGE", use_v=use_v, sched="learned")
         ctx.check(ctx._lib.pb_peel_edge(ctx.handle, h, C.byref(o2), ec_host.data_ptr(), wing_host.data_ptr()),
                   "pb_peel_edge")
         ctx._lib.pb_graph_destroy(h)
@@ -264,31 +301,39 @@ def our_arm(args, rank, world, local):
 
     # ---- roofline of the dominant kernel ------------------------------------------------------------
     peak, peak_kind = measured_peaks()
-    peel_share = statistics.mean(peel_ms) / (ms_step)
+    peel_share = peel_ms / ms_step
     n = g.nv + g.nu
     if peel_share >= 0.5:
         # wing peeling: 4 B per probed neighbour id (the enumerated two-hop entries)
         alg_bytes = 4.0 * s2["peel_work"]
-        dur = statistics.mean(peel_ms) / 1e3
+        dur = peel_ms / 1e3
         kern = "peel_kernel<wing> (persistent cooperative wing peeling)"
     else:
         alg_bytes = 4.0 * w_rank + 4.0 * (n + 1) + 4.0 * 2 * g.m + 8.0 * g.m
-        dur = statistics.mean(agg_ms) / 1e3
+        dur = agg_ms / 1e3
         kern = "count_warp_kernel + count_block_kernel (wedge aggregation)"
     achieved = alg_bytes / dur / 1e9
     agg_bytes = 4.0 * w_rank + 4.0 * (n + 1) + 4.0 * 2 * g.m + 8.0 * g.m
-    agg_gbs = agg_bytes / (statistics.mean(agg_ms) / 1e3) / 1e9
+    agg_gbs = agg_bytes / (agg_ms / 1e3) / 1e9
 
     line = {
         "metric": "wedges/s", "value": value, "unit": "wedges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded R-MAT generator)",
-        "config": dict(WORKLOAD, w_rank=w_rank, w_side=w_side, parallelism=f"replicas x{world}"),
-        "count_ms": statistics.mean(count_ms), "peel_ms": statistics.mean(peel_ms),
-        "count_wedges_per_s": w_rank / (statistics.mean(count_ms) / 1e3),
+        "config": dict(WORKLOAD, w_rank=w_rank, w_side=w_side, parallelism=f"replicas x{world}",
+                       sched="learned (value); plain timed in the same run"),
+        "plain": {"value": plain_value, "ms_per_step": plain["ms_step"], "count_ms": plain["count_ms"],
+                  "peel_ms": plain["peel_ms"], "agg_ms": plain["agg_ms"], "gpu_launches": plain["launches"]},
+        "learned_over_plain": value / plain_value,
+        "sched": {"model": model_info, "count_items": s1["sched_items"], "count_ms_sched": s1["ms_sched"],
+                  "count_pred_cycles": s1["sched_pred"], "count_meas_cycles": s1["sched_meas"],
+                  "count_mae_log2": s1["sched_mae_log2"], "peel_choice": s2["sched_choice"],
+                  "peel_pred_ms": s2["sched_pred"], "peel_meas_ms": s2["sched_meas"],
+                  "peel_ms_sched": s2["ms_sched"]},
+        "count_ms": count_ms, "peel_ms": peel_ms,
+        "count_wedges_per_s": w_rank / (count_ms / 1e3),
         "peel_rounds": s2["peel_rounds"], "peel_work": s2["peel_work"],
-        "aggregation": {"ms": statistics.mean(agg_ms), "alg_bytes": agg_bytes, "achieved_gbs": agg_gbs,
-                        "frac": agg_gbs / peak},
+        "aggregation": {"ms": agg_ms, "alg_bytes": agg_bytes, "achieved_gbs": agg_gbs, "frac": agg_gbs / peak},
         "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
         "e2e": {"value": w_rank * world / (e2e_ms / 1e3), "unit": "wedges/s", "ms_per_step": e2e_ms,

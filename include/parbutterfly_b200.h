@@ -61,7 +61,10 @@ typedef struct {
   int64_t max_wedges;     /* -m, default 2577500000 (BipartiteButterflies.C:172) */
   int64_t max_array_size; /* -a, default 23090996160 (BipartiteButterflies.C:173) */
   int32_t sched;          /* pb_sched, default PB_SCHED_PLAIN */
-  int32_t autotune;       /* 0/1: let the autotuner pick tile/batch/table sizes */
+  int32_t autotune;       /* 0/1: the autotuner picks the block aggregator's table size, CTAs
+                             per SM and warp/CTA boundary per graph: the first call on a graph
+                             signature times every candidate, later calls on the context reuse
+                             the fastest (results are identical either way) */
   int32_t use_v;          /* -1 = choose as cmpWedgeCounts does; 0/1 forces the count side */
   int32_t reserved;
 } pb_opts;
@@ -109,6 +112,11 @@ typedef struct {
   double sched_pred;      /* predicted time: SM cycles summed over items (count), ms (peel) */
   double sched_meas;      /* measured time in the same unit */
   double sched_mae_log2;  /* count calls: mean |log2(predicted / measured)| over the items */
+  /* Block-aggregator geometry of the last count call (opts.autotune picks it per graph): */
+  int32_t count_smem_bytes;    /* shared-memory table bytes per CTA */
+  int32_t count_blocks_per_sm; /* CTAs per SM */
+  int32_t count_small_w;       /* endpoints with at most this many wedges go to a warp */
+  int32_t autotuned;           /* 1 when this call ran the autotuner's sweep */
 } pb_stats;
 
 typedef struct pb_ctx pb_ctx;
@@ -223,6 +231,22 @@ pb_status pb_trace_clear(pb_ctx* ctx);
  * strides, A(m,k) = A[m*sam + k*sak], B(n,k) = B[n*sbn + k*sbk]; 1 <= N <= 128. */
 pb_status pb_tc_gemm_bf16(pb_ctx* ctx, int64_t M, int32_t N, int64_t K, const void* A, int64_t sam, int64_t sak,
                           const void* B, int64_t sbn, int64_t sbk, float* D, int64_t ldd);
+
+/* ---- a batch as one CUDA graph (no counterpart in the reference) ----------------------------
+ * Count (butterfly_count.h:1634-1731) and Peel (butterfly_peel.h:896-934) of k graphs, planned
+ * once and replayed as one CUDA graph: pb_batch_create builds the disjoint union on the device
+ * (each graph's count side as cmpWedgeCounts decides for it), runs the whole pipeline once
+ * eagerly (ranking, per-vertex counting, tip peeling as one persistent launch) while logging
+ * every host readback, then captures the same sequence with the logged values, so the graph
+ * holds no host synchronisation.  opts.autotune tunes the aggregator geometry on the union
+ * first.  pb_batch_run replays the graph (the full ranking + counting + peeling work every
+ * time) and copies counts[g] / tips[g] (nCount(g) each, host or device; either may be NULL) out;
+ * stats.ms_count is the replay's device time.  Count types HASH/AHASH/BATCHS/BATCHWA/SERIAL
+ * (SORT / HIST return PB_EUNSUPPORTED).  The graphs may be destroyed after pb_batch_create. */
+typedef struct pb_batch pb_batch;
+pb_status pb_batch_create(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts, pb_batch** out);
+pb_status pb_batch_run(pb_ctx* ctx, pb_batch* batch, int64_t* const* counts, int64_t* const* tips);
+pb_status pb_batch_destroy(pb_batch* batch);
 
 /* ---- counting without device allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc where they need a

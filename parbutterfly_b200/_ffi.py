@@ -27,7 +27,8 @@ EXPORTS = [
     "pb_gen_powerlaw_u", "pb_gen_zipf", "pb_gen_batch_member", "pb_count_total_noalloc",
     "pb_count_vert_batch", "pb_peel_vert_batch", "pb_sched_model_create", "pb_sched_model_destroy",
     "pb_sched_train", "pb_sched_predict", "pb_sched_save", "pb_sched_load", "pb_ctx_set_sched_model",
-    "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16",
+    "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16", "pb_batch_create", "pb_batch_run",
+    "pb_batch_destroy",
 ]
 
 SCHED_FEATURES = 16
@@ -71,7 +72,8 @@ class Stats(C.Structure):
         ("peel_rounds", C.c_int64), ("peel_work", C.c_int64), ("ms_agg_kernel", C.c_double),
         ("sched_used", C.c_int32), ("sched_choice", C.c_int32), ("sched_items", C.c_int64),
         ("ms_sched", C.c_double), ("sched_pred", C.c_double), ("sched_meas", C.c_double),
-        ("sched_mae_log2", C.c_double),
+        ("sched_mae_log2", C.c_double), ("count_smem_bytes", C.c_int32), ("count_blocks_per_sm", C.c_int32),
+        ("count_small_w", C.c_int32), ("autotuned", C.c_int32),
     ]
 
 
@@ -132,6 +134,9 @@ def lib():
         "pb_trace_rows": (S, [P, I32, P, P, I64, C.POINTER(I64)]),
         "pb_trace_clear": (S, [P]),
         "pb_tc_gemm_bf16": (S, [P, I64, I32, I64, P, I64, I64, P, I64, I64, P, I64]),
+        "pb_batch_create": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
+        "pb_batch_run": (S, [P, P, C.POINTER(P), C.POINTER(P)]),
+        "pb_batch_destroy": (S, [P]),
     }
     for name, (res, args) in sig.items():
         try:

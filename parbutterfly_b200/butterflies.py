@@ -240,6 +240,41 @@ def peel_batch(dgs, counts, peel_type="BATCHS", **kw):
     return [t[:c.size] for t, c in zip(tips, cs)]
 
 
+class BatchGraph:
+    """k graphs planned as one CUDA graph (pb_batch): every run() replays ranking, per-vertex
+    counting and tip peeling of the whole batch and returns (counts, tips) per graph."""
+
+    def __init__(self, dgs, count_type="BATCHS", rank_type="ADEG", **kw):
+        self.ctx = dgs[0].ctx
+        self.sides = [(dg.nu if cmp_wedge_counts(dg)[0] else dg.nv) for dg in dgs]
+        self._h = C.c_void_p()
+        k = len(dgs)
+        hs = (C.c_void_p * k)(*[dg.handle for dg in dgs])
+        o = make_opts(count_type, rank_type, per="VERT", **kw)
+        self.ctx.check(self.ctx._lib.pb_batch_create(self.ctx.handle, hs, k, C.byref(o), C.byref(self._h)),
+                       "pb_batch_create")
+        self.counts = [np.zeros(max(n, 1), dtype=np.int64) for n in self.sides]
+        self.tips = [np.zeros(max(n, 1), dtype=np.int64) for n in self.sides]
+
+    def run(self, copy_out=True):
+        k = len(self.sides)
+        pc = (C.c_void_p * k)(*[c.ctypes.data for c in self.counts]) if copy_out else None
+        pt = (C.c_void_p * k)(*[t.ctypes.data for t in self.tips]) if copy_out else None
+        self.ctx.check(self.ctx._lib.pb_batch_run(self.ctx.handle, self._h, pc, pt), "pb_batch_run")
+        return [c[:n] for c, n in zip(self.counts, self.sides)], [t[:n] for t, n in zip(self.tips, self.sides)]
+
+    def close(self):
+        if self._h:
+            self.ctx._lib.pb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class SchedModel:
     """The learned scheduler's cost models (a pb_sched_model): one for the per-item aggregation
     modes of counting, one for the work-unit setting of peeling."""

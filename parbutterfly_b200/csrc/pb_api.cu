@@ -1,6 +1,10 @@
 // C ABI of libpbgpu: contexts, graphs and the Count / CountE / CountTotal / Peel / PeelE
 // entry points (include/parbutterfly_b200.h).
 #include <algorithm>
+#include <array>
+#include <map>
+#include <memory>
+#include <tuple>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -20,6 +24,25 @@ struct pb_sched_model {
   pb::MlpModel count, peel;
 };
 
+// A planned batch: the disjoint union of k graphs and one CUDA graph that ranks it, counts its
+// butterflies per vertex and peels its tips (pb_batch_create / pb_batch_run).
+struct pb_batch {
+  int device = 0;
+  pb_graph U;
+  std::vector<int64_t> kbase, ksize;
+  pb::DevBuf<int64_t> counts, tips;  // union count side (U side of the union)
+  pb::Recorder rec;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int rank_type = PB_ADEG, strategy = 0;
+  std::array<int, 3> geom = {0, 0, 0};
+  bool tuned = false;
+  ~pb_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
 struct pb_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -29,6 +52,8 @@ struct pb_ctx {
   int64_t launches = 0;
   // Learned scheduler: attached model and trace log (index: pb_sched_target).
   pb_sched_model* model = nullptr;
+  // Autotuner: block-aggregator geometry per graph signature (n, 2m, W_rank, per type).
+  std::map<std::tuple<int64_t, int64_t, int64_t, int>, std::array<int, 3>> tuned;
   int trace_mode = PB_TRACE_OFF;
   uint64_t trace_seed = 0;
   uint64_t peel_sweep[2] = {0, 0};  // explore-mode position in the setting grid (tip, wing)
@@ -38,6 +63,33 @@ struct pb_ctx {
 namespace pb {
 
 thread_local int64_t* g_launch_counter = nullptr;
+thread_local Recorder* g_recorder = nullptr;
+
+Recorder::~Recorder() {
+  for (void* p : pinned) cudaFreeHost(p);
+}
+
+void* Recorder::pinned_alloc(size_t bytes) {
+  void* p = nullptr;
+  PB_CUDA_TRY(cudaMallocHost(&p, bytes));
+  std::memset(p, 0, bytes);
+  pinned.push_back(p);
+  return p;
+}
+
+void readback(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  Recorder* r = g_recorder;
+  if (r && r->capturing) {
+    PB_REQUIRE(r->pos < r->log.size() && r->log[r->pos].size() == bytes, PB_ECUDA,
+               "graph capture: the pipeline took a different path than its recording run");
+    std::memcpy(dst, r->log[r->pos].data(), bytes);
+    ++r->pos;
+    return;
+  }
+  PB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  if (r) r->log.emplace_back((const uint8_t*)dst, (const uint8_t*)dst + bytes);
+}
 
 int sm_count() {
   static int cached[64] = {0};
@@ -228,6 +280,47 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
     hooks.seed = ctx->trace_seed++;
   }
   if (hooks.model || hooks.trace_X) cfg.sched = &hooks;
+  // Autotuner: the first call on a graph signature times the block aggregator under each
+  // candidate geometry (shared-memory table bytes, CTAs per SM, warp/CTA boundary in wedges)
+  // with the plain rule and keeps the fastest for this and later calls on the context.
+  st.autotuned = 0;
+  if (fused && o.autotune && R.w_rank > 0) {
+    static const int kGeom[10][3] = {{48 << 10, 4, 512}, {32 << 10, 4, 512}, {48 << 10, 2, 512}, {96 << 10, 2, 512},
+                                     {200 << 10, 1, 512}, {48 << 10, 4, 256}, {32 << 10, 4, 256},
+                                     {48 << 10, 2, 256}, {96 << 10, 2, 256}, {200 << 10, 1, 256}};
+    const auto key = std::make_tuple(R.n, R.m2, R.w_rank, per);
+    auto it = ctx->tuned.find(key);
+    if (it == ctx->tuned.end()) {
+      DevBuf<int64_t> scratch;
+      int64_t* tgt = per == PB_VERT ? nullptr : out_dev;
+      if (per == PB_VERT) {
+        scratch.alloc(R.n > 0 ? R.n : 1, s);
+        tgt = scratch.get();
+      }
+      double best = 1e300;
+      std::array<int, 3> bg = {kGeom[0][0], kGeom[0][1], kGeom[0][2]};
+      for (const auto& gm : kGeom) {
+        CountConfig t = cfg;
+        t.sched = nullptr;
+        t.smem_bytes = gm[0];
+        t.blocks_per_sm = gm[1];
+        t.small_w = gm[2];
+        const CountResult r = count_ranked(R, per, tgt, t, s);
+        if (r.agg_ms < best) {
+          best = r.agg_ms;
+          bg = {gm[0], gm[1], gm[2]};
+        }
+      }
+      it = ctx->tuned.emplace(key, bg).first;
+      st.autotuned = 1;
+    }
+    cfg.smem_bytes = it->second[0];
+    cfg.blocks_per_sm = it->second[1];
+    cfg.small_w = it->second[2];
+  }
+  st.count_smem_bytes = cfg.smem_bytes;
+  st.count_blocks_per_sm = cfg.blocks_per_sm;
+  st.count_small_w = cfg.small_w;
   DevBuf<uint32_t> chk;
   if (check_mode()) {
     chk.alloc(4, s);
@@ -281,6 +374,30 @@ void run_count(pb_ctx* ctx, const pb_graph* g, const pb_opts& o, int per, int us
   st.sched_pred = hooks.pred_cycles;
   st.sched_meas = hooks.meas_cycles;
   st.sched_mae_log2 = hooks.mae_log2;
+}
+
+// The batch pipeline of pb_batch_create: rank the union (count side = U), count per vertex,
+// gather the counts to union ids, peel tips.  Host readbacks go through readback(), so the same
+// sequence records (eagerly) and then captures into a CUDA graph.
+void batch_pipeline(pb_batch& b, cudaStream_t s) {
+  const pb_graph& U = b.U;
+  Ranked R;
+  vertex_order(U, b.rank_type, 1, R, s);
+  build_ranked_csr(U, R, false, s);
+  wedge_scan(R, s);
+  CountConfig cfg;
+  cfg.strategy = b.strategy;
+  if (b.tuned) {
+    cfg.smem_bytes = b.geom[0];
+    cfg.blocks_per_sm = b.geom[1];
+    cfg.small_w = b.geom[2];
+  }
+  DevBuf<int64_t> rc(R.n > 0 ? R.n : 1, s);
+  count_ranked(R, PB_VERT, rc.get(), cfg, s);
+  if (U.nu > 0)
+    PB_LAUNCH(gather_vert_kernel, std::max(1, std::min(ceil_div(U.nu, 256), sm_count() * 8)), 256, 0, s, rc.get(),
+              R.rank.get(), U.nv, U.nu, b.counts.get());
+  peel_vertices(U, 1, b.counts.get(), b.tips.get(), s, plain_peel_tuning(false));
 }
 
 // Work-unit setting of one peel call: learned (when a trained model is attached and the call
@@ -656,6 +773,107 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
     ctx->stats.sched_meas = ctx->stats.ms_peel;
     log_peel_trace(ctx, row, ctx->stats.ms_peel);
   });
+}
+
+pb_status pb_batch_create(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, const pb_opts* opts, pb_batch** out) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(gs && out && k > 0, PB_EINVAL, "null argument or empty batch");
+    *out = nullptr;
+    pb_opts o = resolve_opts(opts);
+    PB_REQUIRE(o.count_type != PB_SORT && o.count_type != PB_ASORT && o.count_type != PB_HIST &&
+                   o.count_type != PB_AHIST,
+               PB_EUNSUPPORTED, "batch graphs run the fused aggregators (HASH / BATCHS / BATCHWA / SERIAL)");
+    cudaStream_t s = ctx->stream;
+    std::unique_ptr<pb_batch> b(new pb_batch());
+    b->device = ctx->device;
+    b->rank_type = o.rank_type;
+    b->strategy = (o.count_type == PB_HASH || o.count_type == PB_AHASH) ? STRAT_HASH : STRAT_DENSE;
+    build_union(gs, k, b->U, b->kbase, b->ksize, s);
+    const int64_t n = b->U.nu;
+    b->counts.alloc(n > 0 ? n : 1, s);
+    b->tips.alloc(n > 0 ? n : 1, s);
+    if (o.autotune) {  // tune the aggregator geometry on the union once, eagerly
+      pb_opts t = o;
+      t.use_v = 1;
+      t.sched = PB_SCHED_PLAIN;
+      run_count(ctx, &b->U, t, PB_VERT, 1, b->counts.get());
+      b->geom = {ctx->stats.count_smem_bytes, ctx->stats.count_blocks_per_sm, ctx->stats.count_small_w};
+      b->tuned = true;
+    }
+    b->rec.status = (unsigned*)b->rec.pinned_alloc(2 * sizeof(unsigned));
+    // 1. Recording run (eager): every host readback is logged.
+    g_recorder = &b->rec;
+    try {
+      batch_pipeline(*b, s);
+      PB_CUDA_TRY(cudaStreamSynchronize(s));
+      // 2. Capture: the same sequence, readbacks served from the log.
+      b->rec.capturing = true;
+      b->rec.pos = 0;
+      PB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      try {
+        batch_pipeline(*b, s);
+      } catch (...) {
+        cudaGraph_t broken = nullptr;
+        cudaStreamEndCapture(s, &broken);
+        if (broken) cudaGraphDestroy(broken);
+        throw;
+      }
+      PB_CUDA_TRY(cudaStreamEndCapture(s, &b->graph));
+    } catch (...) {
+      g_recorder = nullptr;
+      b->rec.capturing = false;
+      throw;
+    }
+    g_recorder = nullptr;
+    b->rec.capturing = false;
+    PB_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    *out = b.release();
+  });
+}
+
+pb_status pb_batch_run(pb_ctx* ctx, pb_batch* b, int64_t* const* counts, int64_t* const* tips) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(b && b->exec, PB_EINVAL, "null batch");
+    PB_REQUIRE(b->device == ctx->device, PB_EINVAL, "batch and context are on different devices");
+    cudaStream_t s = ctx->stream;
+    Timer T(s);
+    b->rec.status[0] = 0xFFFFFFFFu;
+    T.mark();
+    PB_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    T.mark();
+    const int k = (int)b->kbase.size();
+    for (int g = 0; g < k; ++g) {
+      if (!b->ksize[g]) continue;
+      const size_t bytes = sizeof(int64_t) * b->ksize[g];
+      if (counts && counts[g])
+        PB_CUDA_TRY(cudaMemcpyAsync(counts[g], b->counts.get() + b->kbase[g], bytes, cudaMemcpyDefault, s));
+      if (tips && tips[g])
+        PB_CUDA_TRY(cudaMemcpyAsync(tips[g], b->tips.get() + b->kbase[g], bytes, cudaMemcpyDefault, s));
+    }
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (b->U.nu > 0) {
+      const unsigned err = b->rec.status[0], alive = b->rec.status[1];
+      PB_REQUIRE(err != 0xFFFFFFFFu, PB_ECUDA, "batch graph: the peel reported no status");
+      PB_REQUIRE(!(err & 1u), PB_ETIMEOUT, "batch graph: a grid barrier wait of the peel ran out of time");
+      PB_REQUIRE(err == 0 && alive == 0, PB_ECUDA, "batch graph: peeling did not complete");
+    }
+    std::memset(&ctx->stats, 0, sizeof(ctx->stats));
+    ctx->stats.ms_count = T.ms(0, 1);  // the whole replay: ranking, counting and peeling
+    ctx->stats.count_smem_bytes = b->geom[0];
+    ctx->stats.count_blocks_per_sm = b->geom[1];
+    ctx->stats.count_small_w = b->geom[2];
+  });
+}
+
+pb_status pb_batch_destroy(pb_batch* b) {
+  if (!b) return PB_EINVAL;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  delete b;
+  cudaSetDevice(prev);
+  return PB_OK;
 }
 
 pb_status pb_peel_vert(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts, const int64_t* counts, int64_t* tip) {

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/parbutterfly_b200.h"
 
@@ -85,6 +86,24 @@ struct DevBuf {
 };
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Host readbacks between kernels (sizes, counters, status words) go through readback(), so a
+// whole pipeline can be captured into a CUDA graph: during an eager recording run every value
+// read is logged; while the stream is being captured the logged values are returned instead
+// and no device-to-host copy or synchronisation enters the graph.  Without an active
+// recorder readback() is a plain cudaMemcpyAsync + cudaStreamSynchronize.
+struct Recorder {
+  bool capturing = false;
+  std::vector<std::vector<uint8_t>> log;
+  size_t pos = 0;
+  std::vector<void*> pinned;  // host memory the captured graph reads or writes (kept alive)
+  unsigned* status = nullptr; // pinned {peel error bits, unpeeled items} written by the graph
+  ~Recorder();
+  void* pinned_alloc(size_t bytes);
+};
+extern thread_local Recorder* g_recorder;
+void readback(void* dst, const void* src, size_t bytes, cudaStream_t s);
+inline bool capturing() { return g_recorder && g_recorder->capturing; }
 
 // Number of SMs of the current device (cached per process; one device per context).
 int sm_count();

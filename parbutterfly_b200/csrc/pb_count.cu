@@ -574,8 +574,14 @@ __global__ void item_features_kernel(Params P, const uint32_t* __restrict__ item
       f[10] = P.out32 ? 1.f : 0.f;
       f[11] = log2f(1.f + (float)W / (float)(deg ? deg : 1u));
       for (int k = kItemFeatures; k < kMlpIn; ++k) f[k] = 0.f;
-      valid[q] = (uint8_t)((i <= cap_dense ? 1u : 0u) | ((uint64_t)2 * W <= cap_hash ? 2u : 0u) | 4u |
-                           (2ull * hi_c <= hy_hash ? 8u : 0u));
+      const bool dense_ok = i <= cap_dense, hash_ok = (uint64_t)2 * W <= cap_hash, hybrid_ok = 2ull * hi_c <= hy_hash;
+      // The plain rule's choice (count_block_kernel) rides in the top bits.
+      const uint32_t rule = (dense_ok && (uint64_t)i <= 4ull * (uint64_t)W) ? MODE_DENSE
+                            : hash_ok                                     ? MODE_HASH
+                            : dense_ok                                    ? MODE_DENSE
+                            : hybrid_ok                                   ? MODE_HYBRID
+                                                                          : MODE_GLOBAL;
+      valid[q] = (uint8_t)((dense_ok ? 1u : 0u) | (hash_ok ? 2u : 0u) | 4u | (hybrid_ok ? 8u : 0u) | (rule << 4));
     }
   }
 }
@@ -596,17 +602,26 @@ __global__ void sched_candidates_kernel(const float* __restrict__ F, uint32_t n_
   }
 }
 
-// The valid shared-memory mode with the least predicted log2 cycles, else the global mode.
+// The valid shared-memory mode with the least predicted log2 cycles; the plain rule's mode is
+// kept unless another one is predicted at least kSchedMargin (log2 units, 10%) cheaper.  Items
+// no shared-memory mode can hold take the global mode.
+constexpr float kSchedMargin = 0.1375f;
 __global__ void sched_choose_kernel(const float* __restrict__ y, const uint8_t* __restrict__ valid, uint32_t n_items,
                                     uint8_t* modes, float* pred, uint32_t* n_global) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t vq = valid[q], rule = vq >> 4;
     int best = MODE_GLOBAL;
-    float by = 1e30f;
+    float by = 1e30f, ry = 1e30f;
     for (int c = 0; c < 3; ++c) {
       const int m = kCandMode[c];
-      if (!(valid[q] & (1u << m))) continue;
+      if (!(vq & (1u << m))) continue;
       const float v = y[q * 3 + c];
       if (v < by) { by = v; best = m; }
+      if ((uint32_t)m == rule) ry = v;
+    }
+    if (rule != MODE_GLOBAL && ry - by < kSchedMargin) {
+      best = (int)rule;
+      by = ry;
     }
     modes[q] = (uint8_t)best;
     pred[q] = best == MODE_GLOBAL ? -1.f : by;  // no prediction for the fallback
@@ -624,7 +639,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 __global__ void sched_explore_kernel(const uint8_t* __restrict__ valid, uint32_t n_items, uint64_t seed,
                                      uint8_t* modes, uint32_t* n_global) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t vm = valid[q];
+    const uint32_t vm = valid[q] & 15u;
     const uint32_t c = __popc(vm);
     uint32_t k = (uint32_t)(mix64(seed + 0x9E3779B97F4A7C15ull * (uint64_t)(q + 1)) % c);
     int m = 0;
@@ -696,14 +711,15 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   PB_LAUNCH(classify_endpoints_kernel, std::max(1, std::min(ceil_div(n, 256), sms * 8)), 256, 0, s, R.wsum.get(), n,
             small_w, cap_dense, cap_hash, items.get(), counts.get());
   uint32_t hc[2];
-  PB_CUDA_TRY(cudaMemcpyAsync(hc, counts.get(), sizeof(hc), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  readback(hc, counts.get(), sizeof(hc), s);
   res.n_big = (int)hc[0];
 
+  // Under graph capture nothing is timed or read back here (the recording run checked).
+  const bool cap = capturing();
   cudaEvent_t e0, e1;
   PB_CUDA_TRY(cudaEventCreate(&e0));
   PB_CUDA_TRY(cudaEventCreate(&e1));
-  PB_CUDA_TRY(cudaEventRecord(e0, s));
+  if (!cap) PB_CUDA_TRY(cudaEventRecord(e0, s));
   {
     const int smem = kWarpsPerBlockSmall * 2 * kWarpTable * (int)sizeof(uint32_t);
     static bool attr_set = false;
@@ -776,6 +792,11 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   }
   if (P.out32)
     PB_LAUNCH(widen_u32_kernel, std::max(1, std::min(ceil_div(out_len, 256), sms * 8)), 256, 0, s, P.out32, out_len, out);
+  if (cap) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return res;
+  }
   PB_CUDA_TRY(cudaEventRecord(e1, s));
   PB_CUDA_TRY(cudaEventSynchronize(e1));
   {

@@ -1246,8 +1246,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     PB_CUDA_TRY(cudaMemsetAsync(mx.get(), 0, sizeof(unsigned long long), s));
     PB_LAUNCH(max_i64_kernel, grid_for(G.nK), 256, 0, s, wk.get(), G.nK, mx.get());
     unsigned long long hmx = 0;
-    PB_CUDA_TRY(cudaMemcpyAsync(&hmx, mx.get(), sizeof(hmx), cudaMemcpyDeviceToHost, s));
-    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    readback(&hmx, mx.get(), sizeof(hmx), s);
     need_scratch = 2ull * hmx > (uint64_t)kBlockSlots;
     scratch_len = G.nK;
   }
@@ -1299,6 +1298,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.alen[0] = (unsigned)N;
   hctl.alive_at_compact = (unsigned)N;
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
+  // A recorded / captured pipeline runs the peel as one launch without list compaction (the
+  // host cannot step in between launches of a CUDA graph).
+  const bool graph_mode = g_recorder != nullptr;
+  if (graph_mode) hctl.min_gain = 0xFFFFFFFFu;
   hctl.barrier_timeout_ns = kBarrierTimeoutNs;
   hctl.near_min = (unsigned)tune.near_min;
   hctl.near_div = (unsigned)tune.near_div;
@@ -1311,7 +1314,15 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
   DevBuf<Ctl> ctl(1, s);
-  PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  if (capturing()) {
+    // The graph copies from host memory that outlives it; the status words come back to a
+    // pinned buffer the caller checks after every replay.
+    Ctl* h0 = (Ctl*)g_recorder->pinned_alloc(sizeof(Ctl));
+    std::memcpy(h0, &hctl, sizeof(Ctl));
+    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), h0, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  } else {
+    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  }
   Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
@@ -1320,6 +1331,15 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   Ctl* ctl_ptr = ctl.get();
   int launches = 0;
+  if (capturing()) {
+    void* args[] = {&G, &W, &ctl_ptr, &cls};
+    PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
+    if (g_launch_counter) ++*g_launch_counter;
+    // {err, alive} of the control block into the recorder's status slot (pinned).
+    PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status, &ctl_ptr->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status + 1, &ctl_ptr->alive, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    return res;
+  }
   while (true) {
     void* args[] = {&G, &W, &ctl_ptr, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));

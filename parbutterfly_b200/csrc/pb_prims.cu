@@ -360,15 +360,13 @@ void segmented_sort_rows(const uint32_t* off, int64_t nrows, uint32_t* keys, uin
   PB_LAUNCH(rowsort_block_kernel, sms * 4, 512, 0, s, off, mid_rows, cnt.get(), keys, vals);
   if (max_row <= (uint32_t)kRowBlockMax) return;
   uint32_t nbig = 0;
-  PB_CUDA_TRY(cudaMemcpyAsync(&nbig, cnt.get() + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  readback(&nbig, cnt.get() + 1, sizeof(uint32_t), s);
   if (nbig == 0) return;
   DevBuf<uint32_t> tstart(nbig + 1, s);
   PB_LAUNCH(big_row_sizes_kernel, ceil_div(nbig, 256), 256, 0, s, off, big_rows, nbig, tstart.get());
   exclusive_scan_u32(tstart.get(), tstart.get(), nbig, s);
   uint32_t tot = 0;
-  PB_CUDA_TRY(cudaMemcpyAsync(&tot, tstart.get() + nbig, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  readback(&tot, tstart.get() + nbig, sizeof(uint32_t), s);
   DevBuf<uint64_t> tk(tot, s), tk2(tot, s);
   DevBuf<uint32_t> tv, tv2;
   if (vals) { tv.alloc(tot, s); tv2.alloc(tot, s); }

@@ -276,8 +276,7 @@ void cmp_wedge_counts(const pb_graph& g, int* use_v, int64_t* w_min, int64_t* wv
   if (g.nv) PB_LAUNCH(side_wedges_kernel, grid_for(g.nv), 256, 0, s, g.offV.get(), g.nv, acc.get());
   if (g.nu) PB_LAUNCH(side_wedges_kernel, grid_for(g.nu), 256, 0, s, g.offU.get(), g.nu, acc.get() + 1);
   unsigned long long h[2];
-  PB_CUDA_TRY(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  readback(h, acc.get(), sizeof(h), s);
   *wv = (int64_t)h[0];
   *wu = (int64_t)h[1];
   *use_v = *wv <= *wu;
@@ -305,8 +304,7 @@ void vertex_order(const pb_graph& g, int rank_type, int use_v, Ranked& R, cudaSt
       PB_CUDA_TRY(cudaMemsetAsync(kbuf.get(), 0, sizeof(uint32_t), s));
       PB_LAUNCH(cocore_max_kernel, grid_for(n), 256, 0, s, key.get(), done.get(), n, kbuf.get());
       uint32_t k1 = 0;
-      PB_CUDA_TRY(cudaMemcpyAsync(&k1, kbuf.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-      PB_CUDA_TRY(cudaStreamSynchronize(s));
+      readback(&k1, kbuf.get(), sizeof(uint32_t), s);
       if (k1 == 0) break;
       kmax = std::max(kmax, k1 - 1);
       PB_LAUNCH(cocore_round_kernel, grid_for(n * 32), 256, 0, s, lists_of(g), n, approx, kbuf.get(), key.get(),
@@ -366,8 +364,7 @@ void wedge_scan(Ranked& R, cudaStream_t s) {
   PB_LAUNCH(wedge_scan_kernel, grid_for(n * 32), 256, 0, s, R.off.get(), R.adj.get(), below.get(), n, R.pref.get(),
             wc.get());
   exclusive_scan_i64(wc.get(), R.wsum.get(), n, s);
-  PB_CUDA_TRY(cudaMemcpyAsync(&R.w_rank, R.wsum.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  readback(&R.w_rank, R.wsum.get() + n, sizeof(int64_t), s);
 }
 
 bool check_mode() {

@@ -48,3 +48,44 @@ def test_batch_members_match_single_calls(ctx):
         single = pb.count(dg, "HASH", "ADEG")
         np.testing.assert_array_equal(c, single)
         np.testing.assert_array_equal(t, pb.peel(dg, single))
+
+
+def test_batch_graph_replays_match_oracle(ctx):
+    """The planned CUDA graph (ranking + counting + one persistent peel launch for the whole
+    batch) gives every graph's oracle counts and tip numbers on every replay."""
+    gs = _mixed_graphs()
+    dgs = [ctx.upload(g) for g in gs]
+    bg = pb.BatchGraph(dgs, "BATCHS", "ADEG")
+    for rep in range(3):
+        counts, tips = bg.run()
+        for g, c, t in zip(gs, counts, tips):
+            use_v = oracle.cmp_wedge_counts(g)[0]
+            oc, _ = oracle.count(g, "VERT", "ADEG", use_v=use_v)
+            np.testing.assert_array_equal(c, oc)
+            np.testing.assert_array_equal(t, oracle.peel_vert(g, oc, use_v=use_v)[0])
+    assert ctx.stats()["ms_count"] > 0
+    bg.close()
+
+
+def test_batch_graph_autotuned_cocore_hash(ctx):
+    """ACOCORE ranking (a data-dependent number of bucket rounds, recorded and captured) with
+    the HASH aggregator and autotuned geometry; equals the single-graph calls."""
+    gs = [BipartiteGraph.batch_member(k) for k in range(3, 256, 23)]
+    dgs = [ctx.upload(g) for g in gs]
+    bg = pb.BatchGraph(dgs, "HASH", "ACOCORE", autotune=True)
+    counts, tips = bg.run()
+    counts2, tips2 = bg.run()
+    for dg, c, t, c2, t2 in zip(dgs, counts, tips, counts2, tips2):
+        single = pb.count(dg, "HASH", "ACOCORE")
+        np.testing.assert_array_equal(c, single)
+        np.testing.assert_array_equal(t, pb.peel(dg, single))
+        np.testing.assert_array_equal(c2, c)
+        np.testing.assert_array_equal(t2, t)
+    bg.close()
+
+
+def test_batch_graph_rejects_materialising_aggregators(ctx):
+    dgs = [ctx.upload(BipartiteGraph.uniform(50, 40, 300, 5))]
+    with pytest.raises(pb._ffi.PBError) as ei:
+        pb.BatchGraph(dgs, "SORT", "ADEG")
+    assert ei.value.status == pb._ffi.PB_EUNSUPPORTED

@@ -173,3 +173,22 @@ def test_peel_explore_every_setting_exact_and_learned(ctx):
         assert 0 <= ctx.stats()["sched_choice"] < 21
     finally:
         pb.detach_sched_model(ctx)
+
+
+def test_autotune_picks_a_geometry_once_and_keeps_results(ctx):
+    g = _rmat(61, 12, 11, 60000)
+    dg = ctx.upload(g)
+    plain = pb.count(dg, "HASH", "ADEG")
+    first = pb.count(dg, "HASH", "ADEG", autotune=True)
+    st1 = ctx.stats()
+    again = pb.count(dg, "HASH", "ADEG", autotune=True)
+    st2 = ctx.stats()
+    np.testing.assert_array_equal(first, plain)
+    np.testing.assert_array_equal(again, plain)
+    assert st1["autotuned"] == 1 and st2["autotuned"] == 0
+    geom = (st2["count_smem_bytes"], st2["count_blocks_per_sm"], st2["count_small_w"])
+    assert geom == (st1["count_smem_bytes"], st1["count_blocks_per_sm"], st1["count_small_w"])
+    assert geom[0] in (32 << 10, 48 << 10, 96 << 10, 200 << 10) and geom[2] in (256, 512)
+    e = pb.count_e(dg, "HASH", "ADEG", autotune=True)
+    np.testing.assert_array_equal(e, pb.count_e(dg, "HASH", "ADEG"))
+    assert pb.count_total(dg, "BATCHS", "ADEG", autotune=True) == int(plain.sum()) // 2
