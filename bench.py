@@ -358,6 +358,143 @@ def our_arm(args, rank, world, local):
         print(json.dumps(line))
 
 
+C4 = {
+    "workload": "256 seeded bipartite graphs (graph g: seed 4000+g, |U|,|V| log-uniform in [64, 65536], "
+                "m = log-uniform factor in [4, 64] x min(|U|,|V|), uniform or Zipf-1.5 endpoints by a seeded coin); "
+                "per-vertex BATCHS counts (ADEG rank) + tip peel of every graph",
+    "graphs": 256, "rank_type": "ADEG", "count_type": "BATCHS", "per": "VERT", "peel_type": "BATCHS",
+    "l2": "inputs larger than L2 plus a 256 MiB L2 flush before every timed step",
+}
+
+
+def c4_arm(args, rank, world, local):
+    """The 256-graph batch: one CUDA graph replay (plan built once: union, recorded readbacks,
+    captured ranking + counting + one persistent peel launch; autotuned aggregator geometry)
+    against the per-graph loop of the fixed-strategy path and the union calls."""
+    import numpy as np
+    import torch
+    from parbutterfly_b200 import butterflies as pb
+    from parbutterfly_b200.graph import BipartiteGraph
+
+    graphs = [BipartiteGraph.batch_member(k) for k in range(C4["graphs"])]
+    stream = torch.cuda.Stream(local)
+    torch.cuda.set_stream(stream)
+    ctx = pb.Context(local, stream=stream.cuda_stream)
+    model, model_info = load_or_train_model(ctx, pb)
+    model.attach()
+    dgs = [ctx.upload(g) for g in graphs]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ref_c = pb.count_batch(dgs, C4["count_type"], C4["rank_type"])
+    w_rank = int(ctx.stats()["w_rank"])
+    ref_t = pb.peel_batch(dgs, ref_c)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        l0 = ctx.kernel_launches()
+        durs = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            e1.synchronize()
+            durs.append(e0.elapsed_time(e1))
+        return max_over_ranks(statistics.mean(durs), world), (ctx.kernel_launches() - l0) // args.steps, out
+
+    def loop():
+        cs = [pb.count(dg, C4["count_type"], C4["rank_type"]) for dg in dgs]
+        return cs, [pb.peel(dg, c) for dg, c in zip(dgs, cs)]
+
+    def union(sched):
+        def f():
+            cs = pb.count_batch(dgs, C4["count_type"], C4["rank_type"], sched=sched)
+            return cs, pb.peel_batch(dgs, cs, sched=sched)
+        return f
+
+    t0 = time.perf_counter()
+    bg = pb.BatchGraph(dgs, C4["count_type"], C4["rank_type"], autotune=True)
+    plan_s = time.perf_counter() - t0
+    st_geom = None
+    clocks = ClockSampler(local)
+    ms_loop, l_loop, out_loop = timed(loop)
+    ms_union, l_union, out_union = timed(union("plain"))
+    ms_union_l, l_union_l, out_union_l = timed(union("learned"))
+    clocks.start()
+    ms_graph, l_graph, out_graph = timed(lambda: bg.run())
+    clk = clocks.stop()
+    st_geom = ctx.stats()
+    for outs in (out_loop, out_union, out_union_l, out_graph):
+        for a, b in zip(outs[0], ref_c):
+            assert np.array_equal(a, b), "counts differ between paths"
+        for a, b in zip(outs[1], ref_t):
+            assert np.array_equal(a, b), "tip numbers differ between paths"
+
+    # End to end through the C ABI: host graphs in, host counts / tips out, every step.
+    from parbutterfly_b200 import _ffi
+    import ctypes as C
+
+    def e2e_step():
+        hs = []
+        for g in graphs:
+            s_ = g.csr_struct()
+            h = C.c_void_p()
+            ctx.check(ctx._lib.pb_graph_upload(ctx.handle, C.byref(s_), C.byref(h)), "pb_graph_upload")
+            hs.append(h)
+        k = len(hs)
+        arr = (C.c_void_p * k)(*hs)
+        outs_c = [np.zeros(max(len(c), 1), dtype=np.int64) for c in ref_c]
+        outs_t = [np.zeros(max(len(c), 1), dtype=np.int64) for c in ref_c]
+        pc = (C.c_void_p * k)(*[o.ctypes.data for o in outs_c])
+        pt = (C.c_void_p * k)(*[o.ctypes.data for o in outs_t])
+        o = pb.make_opts(C4["count_type"], C4["rank_type"], per="VERT")
+        ctx.check(ctx._lib.pb_count_vert_batch(ctx.handle, arr, k, C.byref(o), pc), "pb_count_vert_batch")
+        ctx.check(ctx._lib.pb_peel_vert_batch(ctx.handle, arr, k, C.byref(o), pc, pt), "pb_peel_vert_batch")
+        for h in hs:
+            ctx._lib.pb_graph_destroy(h)
+        return outs_c, outs_t
+
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_n = max(1, min(args.steps, 2))
+    for _ in range(e2e_n):
+        oc, ot = e2e_step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_n
+    for a, b in zip(oc, ref_c):
+        assert np.array_equal(a[:len(b)], b)
+    h2d = sum(g.nbytes for g in graphs)
+    d2h = 2 * 8 * sum(len(c) for c in ref_c)
+    line = {
+        "metric": "wedges/s", "value": w_rank * world / (ms_graph / 1e3), "unit": "wedges/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded batch generator)",
+        "config": dict(C4, w_rank=w_rank, m_total=int(sum(g.m for g in graphs)), parallelism=f"replicas x{world}",
+                       path="CUDA graph replay of the planned batch (autotuned geometry)",
+                       geometry={"smem_bytes": st_geom["count_smem_bytes"], "ctas_per_sm": st_geom["count_blocks_per_sm"],
+                                 "warp_max_wedges": st_geom["count_small_w"]}),
+        "plan_s": plan_s,
+        "per_graph_loop": {"ms_per_step": ms_loop, "value": w_rank / (ms_loop / 1e3), "gpu_launches": l_loop},
+        "union_calls": {"ms_per_step": ms_union, "value": w_rank / (ms_union / 1e3), "gpu_launches": l_union},
+        "union_calls_learned": {"ms_per_step": ms_union_l, "value": w_rank / (ms_union_l / 1e3),
+                                "gpu_launches": l_union_l, "model": model_info},
+        "graph_over_loop": ms_loop / ms_graph,
+        "e2e": {"value": w_rank * world / (e2e_ms / 1e3), "unit": "wedges/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "pb_graph_upload x256 + pb_count_vert_batch + pb_peel_vert_batch with host buffers"},
+        "gpu_launches": l_graph,
+        "clocks": clk,
+    }
+    bg.close()
+    for dg in dgs:
+        dg.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -365,11 +502,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                    help="c2: the R-MAT 2^24 count + wing peel (default); c4: the 256-graph batch")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
+        elif args.workload == "c4":
+            c4_arm(args, rank, world, local)
         else:
             our_arm(args, rank, world, local)
     finally:

@@ -37,6 +37,8 @@ struct pb_batch {
   int rank_type = PB_ADEG, strategy = 0;
   std::array<int, 3> geom = {0, 0, 0};
   bool tuned = false;
+  int64_t graph_launches = 0;  // kernel launches one replay performs
+  pb::PeelParts parts;         // one peel instance per graph
   ~pb_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -397,7 +399,17 @@ void batch_pipeline(pb_batch& b, cudaStream_t s) {
   if (U.nu > 0)
     PB_LAUNCH(gather_vert_kernel, std::max(1, std::min(ceil_div(U.nu, 256), sm_count() * 8)), 256, 0, s, rc.get(),
               R.rank.get(), U.nv, U.nu, b.counts.get());
-  peel_vertices(U, 1, b.counts.get(), b.tips.get(), s, plain_peel_tuning(false));
+  peel_vertices(U, 1, b.counts.get(), b.tips.get(), s, plain_peel_tuning(false), &b.parts);
+}
+
+// One peel instance per graph of a batch, weighted by its two-hop work.
+PeelParts batch_parts(const std::vector<int64_t>& kbase, const std::vector<int64_t>& ksize,
+                      const std::vector<double>& work) {
+  PeelParts p;
+  p.base = kbase;
+  p.size = ksize;
+  p.weight = work;
+  return p;
 }
 
 // Work-unit setting of one peel call: learned (when a trained model is attached and the call
@@ -747,7 +759,8 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
     cudaStream_t s = ctx->stream;
     pb_graph U;
     std::vector<int64_t> kbase, ksize;
-    build_union(gs, k, U, kbase, ksize, s);
+    std::vector<double> work;
+    build_union(gs, k, U, kbase, ksize, s, &work);
     const int64_t n = U.nu;
     if (n == 0) return;
     DevBuf<int64_t> cin(n, s), tout(n, s);
@@ -761,7 +774,8 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
     float pred = 0.f;
     const PeelTuning tune = peel_setting(ctx, U, 1, false, cin.get(), o, row, &pred);
     T.mark();
-    PeelResult pr = peel_vertices(U, 1, cin.get(), tout.get(), s, tune);
+    const PeelParts parts = batch_parts(kbase, ksize, work);
+    PeelResult pr = peel_vertices(U, 1, cin.get(), tout.get(), s, tune, &parts);
     T.mark();
     for (int g = 0; g < k; ++g)
       if (ksize[g])
@@ -788,7 +802,9 @@ pb_status pb_batch_create(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, con
     b->device = ctx->device;
     b->rank_type = o.rank_type;
     b->strategy = (o.count_type == PB_HASH || o.count_type == PB_AHASH) ? STRAT_HASH : STRAT_DENSE;
-    build_union(gs, k, b->U, b->kbase, b->ksize, s);
+    std::vector<double> work;
+    build_union(gs, k, b->U, b->kbase, b->ksize, s, &work);
+    b->parts = batch_parts(b->kbase, b->ksize, work);
     const int64_t n = b->U.nu;
     b->counts.alloc(n > 0 ? n : 1, s);
     b->tips.alloc(n > 0 ? n : 1, s);
@@ -810,8 +826,10 @@ pb_status pb_batch_create(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, con
       b->rec.capturing = true;
       b->rec.pos = 0;
       PB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      const int64_t l0 = ctx->launches;
       try {
         batch_pipeline(*b, s);
+        b->graph_launches = ctx->launches - l0;
       } catch (...) {
         cudaGraph_t broken = nullptr;
         cudaStreamEndCapture(s, &broken);
@@ -841,6 +859,7 @@ pb_status pb_batch_run(pb_ctx* ctx, pb_batch* b, int64_t* const* counts, int64_t
     T.mark();
     PB_CUDA_TRY(cudaGraphLaunch(b->exec, s));
     T.mark();
+    ctx->launches += b->graph_launches;
     const int k = (int)b->kbase.size();
     for (int g = 0; g < k; ++g) {
       if (!b->ksize[g]) continue;

@@ -85,9 +85,10 @@ int grid_for(int64_t n) { return std::max(1, std::min(ceil_div(n, 256), sm_count
 
 }  // namespace
 
-// Builds the union graph; returns per-graph count-side bases and sizes.
+// Builds the union graph; returns per-graph count-side bases and sizes, and (when work is not
+// null) each graph's two-hop wedges from its count side, sum over centres of deg (deg - 1).
 void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int64_t>& kbase,
-                 std::vector<int64_t>& ksize, cudaStream_t s) {
+                 std::vector<int64_t>& ksize, cudaStream_t s, std::vector<double>* work) {
   PB_REQUIRE(k > 0, PB_EINVAL, "empty batch");
   std::vector<const uint32_t*> hoffV(k), hoffU(k);
   std::vector<int64_t> hnv(k), hnu(k);
@@ -120,11 +121,13 @@ void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int6
   std::vector<int64_t> kst(k), cst(k);
   kbase.assign(k, 0);
   ksize.assign(k, 0);
+  if (work) work->assign(k, 0.0);
   int64_t nK = 0, nC = 0, m = 0;
   uint32_t maxdeg = 0;
   for (int g = 0; g < k; ++g) {
     const pb_graph* G = gs[g];
     const bool use_v = hs[2 * g] <= hs[2 * g + 1];  // count side U when use_v
+    if (work) (*work)[g] = 2.0 * (double)(use_v ? hs[2 * g] : hs[2 * g + 1]) + (double)G->m;
     GraphRef& R = refs[g];
     R.offK = use_v ? G->offU.get() : G->offV.get();
     R.edgK = use_v ? G->edgU.get() : G->edgV.get();

@@ -95,7 +95,7 @@ CountResult count_ranked_materialized(const Ranked& R, int per, int64_t* out, bo
 // Batches (pb_batch.cu): the disjoint union of k graphs, each graph's count side on the union's
 // U side (count with use_v = 1); kbase/ksize locate each graph's count side in the union.
 void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int64_t>& kbase,
-                 std::vector<int64_t>& ksize, cudaStream_t s);
+                 std::vector<int64_t>& ksize, cudaStream_t s, std::vector<double>* work = nullptr);
 
 // Peeling stage (pb_peel.cu).
 struct PeelResult {
@@ -118,8 +118,15 @@ inline PeelTuning plain_peel_tuning(bool wing) {
   if (!wing) t.huge_work = int64_t(1) << 13;
   return t;
 }
+// Independent peel instances of one launch (the graphs of a batch): items base[i] ..
+// base[i] + size[i] - 1 form instance i, which gets a share of the CTAs in proportion to
+// weight[i] and runs its own rounds.
+struct PeelParts {
+  std::vector<int64_t> base, size;
+  std::vector<double> weight;
+};
 PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s,
-                         const PeelTuning& tune = plain_peel_tuning(false));
+                         const PeelTuning& tune = plain_peel_tuning(false), const PeelParts* parts = nullptr);
 PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s,
                       const PeelTuning& tune = plain_peel_tuning(true));
 

@@ -105,8 +105,16 @@ struct Work {
   uint32_t* gshared;   // grid-shared dense counters / probe markers for huge items (zeroed)
   uint32_t* gscratch;  // per-CTA dense scratch (dense counters / probe markers)
   int64_t gscratch_len;
-  int64_t N;           // items
+  int64_t N;           // items of this instance
+  uint32_t item0;      // first item id of this instance (its items are item0 .. item0 + N - 1)
 };
+
+// Every CTA belongs to one peel instance (the whole input, or one graph of a batch, each with
+// its own control block, lists and rounds): its index within the instance and the instance's
+// CTA count, set at kernel start.
+__shared__ unsigned s_vb, s_vg;
+__device__ __forceinline__ unsigned vblock() { return s_vb; }
+__device__ __forceinline__ unsigned vgrid() { return s_vg; }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -117,7 +125,7 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 // CTA 0 charges the time since its previous mark to phase `ph` (called right after barriers).
 // Phase P is also binned by log2 of the round's estimated work (est).
 __device__ __forceinline__ void phase_mark(Ctl* ctl, int ph, unsigned long long est = 0) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (vblock() == 0 && threadIdx.x == 0) {
     const unsigned long long now = globaltimer_ns();
     if (ctl->t_last) {
       ctl->phase_ns[ph] += now - ctl->t_last;
@@ -132,8 +140,8 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int ph, unsigned long long 
   }
 }
 
-// Grid barrier for a cooperative launch (all CTAs co-resident).  Bounded: a wait longer than
-// kBarrierTimeoutNs sets ERR_TIMEOUT and returns false.
+// Barrier over the CTAs of one peel instance (a cooperative launch keeps every CTA co-resident).
+// Bounded: a wait longer than the control block's timeout sets ERR_TIMEOUT and returns false.
 __device__ bool grid_barrier(Ctl* ctl) {
   __shared__ int ok;
   __syncthreads();
@@ -143,9 +151,9 @@ __device__ bool grid_barrier(Ctl* ctl) {
     __threadfence();
     // (test hook) without CTA 0's arrival no CTA is last, so every wait runs out.
     const unsigned arrived =
-        (blockIdx.x == 0 && *(volatile unsigned*)&ctl->test_skip_arrival) ? 0xFFFFFFFFu : atomicAdd(&ctl->bar_count, 1u);
+        (vblock() == 0 && *(volatile unsigned*)&ctl->test_skip_arrival) ? 0xFFFFFFFFu : atomicAdd(&ctl->bar_count, 1u);
     ok = 1;
-    if (arrived == gridDim.x - 1) {
+    if (arrived == vgrid() - 1) {
       atomicExch(&ctl->bar_count, 0u);
       __threadfence();
       atomicAdd(&ctl->bar_gen, 1u);
@@ -477,8 +485,8 @@ template <int kLevel>
 __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par, const WingEdge& E, uint32_t* keys,
                           uint32_t* vals, uint32_t slots, Shared* S, unsigned long long& work, uint32_t chunk = 0,
                           uint32_t nchunks = 1) {
-  const uint32_t rank = kLevel == LV_WARP ? lane_id() : (kLevel == LV_GRID ? blockIdx.x * kPT + threadIdx.x : threadIdx.x);
-  const uint32_t gsize = kLevel == LV_WARP ? 32 : (kLevel == LV_GRID ? gridDim.x * kPT : kPT);
+  const uint32_t rank = kLevel == LV_WARP ? lane_id() : (kLevel == LV_GRID ? vblock() * kPT + threadIdx.x : threadIdx.x);
+  const uint32_t gsize = kLevel == LV_WARP ? 32 : (kLevel == LV_GRID ? vgrid() * kPT : kPT);
   auto sync = [&]() -> bool {
     if (kLevel == LV_WARP) { __syncwarp(); return true; }
     if (kLevel == LV_BLOCK) { __syncthreads(); return true; }
@@ -535,7 +543,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       block_iter(b, e, *S, first, f);
     } else {
       const uint64_t T = block_total(b, e, *S, first);
-      const uint64_t lo = T * blockIdx.x / gridDim.x, hi = T * (blockIdx.x + 1) / gridDim.x;
+      const uint64_t lo = T * vblock() / vgrid(), hi = T * (vblock() + 1) / vgrid();
       block_iter_range(b, e, *S, first, f, lo, hi);
     }
   };
@@ -629,7 +637,7 @@ __device__ bool tip_item_grid(const Lists& G, const Work& W, Ctl* ctl, unsigned 
     L = G.offC[v + 1] - sb;
   };
   const uint64_t T = (uint64_t)G.wk[u] + (G.offK[u + 1] - G.offK[u]);
-  const uint64_t lo = T * blockIdx.x / gridDim.x, hi = T * (blockIdx.x + 1) / gridDim.x;
+  const uint64_t lo = T * vblock() / vgrid(), hi = T * (vblock() + 1) / vgrid();
   uint32_t* cnt = W.gshared;
   block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
     const uint32_t u2 = G.edgC[q];
@@ -642,7 +650,7 @@ __device__ bool tip_item_grid(const Lists& G, const Work& W, Ctl* ctl, unsigned 
     const int64_t w = atomicExch(&cnt[u2], 0u);
     if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
   }, lo, hi);
-  if (blockIdx.x == 0 && threadIdx.x == 0) work += T;
+  if (vblock() == 0 && threadIdx.x == 0) work += T;
   return grid_barrier(ctl);
 }
 
@@ -697,22 +705,36 @@ struct Classify {
   }
 };
 
+// The peel instances of one launch.  n == 1: the whole grid runs instance 0.  Otherwise CTA b
+// runs instances cta_beg[b] .. cta_end[b] - 1 one after another; instance i spans the ncta[i]
+// CTAs from first[i] (heavy graphs get many CTAs, light graphs share one CTA in turn).
+struct Instances {
+  const Work* W;
+  const uint32_t* first;
+  const uint32_t* ncta;
+  const uint32_t* cta_beg;
+  const uint32_t* cta_end;
+  uint32_t n;
+};
+
+// All rounds of one peel instance, run by its CTAs; false when a bounded wait ran out or an
+// invariant broke (recorded in ctl->err).
 template <bool kWing>
-__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Classify cls) {
+__device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Classify& cls) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Shared& S = *reinterpret_cast<Shared*>(smem_raw);
   uint32_t* pool = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(Shared) + 15) & ~size_t(15)));
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* wkeys = pool + warp * (2 * kWarpSlots);
   uint32_t* wvals = wkeys + kWarpSlots;
-  const unsigned gtid = blockIdx.x * kPT + threadIdx.x;
-  const unsigned gthreads = gridDim.x * kPT;
+  const unsigned gtid = vblock() * kPT + threadIdx.x;
+  const unsigned gthreads = vgrid() * kPT;
   unsigned alist_cur = *(volatile unsigned*)&ctl->alist_cur;
   unsigned long long work = 0;
   if (!*(volatile unsigned*)&ctl->started) {
-    for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = (uint32_t)x;
-    if (!grid_barrier(ctl)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->started = 1;
+    for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = W.item0 + (uint32_t)x;
+    if (!grid_barrier(ctl)) return false;
+    if (vblock() == 0 && threadIdx.x == 0) ctl->started = 1;
   }
 
   for (unsigned long long r = *(volatile unsigned long long*)&ctl->round;; ++r) {
@@ -723,7 +745,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
     // compacted; the host compacts them and relaunches (all CTAs see the same values here).
     const unsigned at_compact = *(volatile unsigned*)&ctl->alive_at_compact;
     if (2u * alive < at_compact && at_compact - alive >= *(volatile unsigned*)&ctl->min_gain) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (vblock() == 0 && threadIdx.x == 0) {
         ctl->round = r;
         ctl->alist_cur = alist_cur;
       }
@@ -751,12 +773,12 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
       if (lane == 0 && mn != kInf) atomicMin(&ctl->k_lo, mn);
       if (threadIdx.x < 66) S.hist[threadIdx.x] = 0;
-      if (blockIdx.x == 0) {
+      if (vblock() == 0) {
         // The previous advance's histogram was last read before two barriers ago.
         if (threadIdx.x < 66) ctl->hist[threadIdx.x] = 0;
         if (threadIdx.x == 0) ctl->near_len = 0;
       }
-      if (!grid_barrier(ctl)) return;
+      if (!grid_barrier(ctl)) return false;
       const unsigned long long klo = *(volatile unsigned long long*)&ctl->k_lo;
       const unsigned alen2 = *(volatile unsigned*)&ctl->alen[na];
       for (unsigned q = gtid; q < alen2; q += gthreads) {
@@ -765,7 +787,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       }
       __syncthreads();
       if (threadIdx.x < 66 && S.hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], S.hist[threadIdx.x]);
-      if (!grid_barrier(ctl)) return;
+      if (!grid_barrier(ctl)) return false;
       // Every CTA derives the same bound: the smallest B with >= target items at distance < 2^B.
       const unsigned target = max(ctl->near_min, alen2 / max(1u, ctl->near_div));
       unsigned cum = 0;
@@ -786,15 +808,15 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
           W.near[atomicAdd(&ctl->near_len, 1u)] = x;
         }
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (vblock() == 0 && threadIdx.x == 0) {
         ctl->win_hi = hi;
         ctl->alen[alist_cur] = 0;  // read by every CTA before the first barrier
         ctl->k_lo = kInf;          // read by every CTA right after the first barrier
       }
       alist_cur = na;
-      if (!grid_barrier(ctl)) return;
+      if (!grid_barrier(ctl)) return false;
       phase_mark(ctl, 0);
-      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->advances += 1;
+      if (vblock() == 0 && threadIdx.x == 0) ctl->advances += 1;
       k = klo;
     }
     const unsigned long long win_hi = *(volatile unsigned long long*)&ctl->win_hi;
@@ -843,7 +865,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
       if (lane == 0 && mn != kInf) atomicMin(&ctl->nm[npar], mn);
-      if (blockIdx.x == 0 && threadIdx.x == 0) {  // slots of the previous round, no longer read
+      if (vblock() == 0 && threadIdx.x == 0) {  // slots of the previous round, no longer read
         ctl->flen_small[npar] = 0;
         ctl->flen_big[npar] = 0;
         ctl->flen_huge[npar] = 0;
@@ -855,11 +877,11 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         ctl->scanned += nl;
       }
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl)) return false;
     phase_mark(ctl, 1);
     // ---- phase P: process the frontier (small items per warp, then heavy items per CTA).
     {
-      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->nm[par] = kInf;  // every CTA has read it
+      if (vblock() == 0 && threadIdx.x == 0) ctl->nm[par] = kInf;  // every CTA has read it
       const unsigned ns = *(volatile unsigned*)&ctl->flen_small[par];
       while (true) {
         unsigned q = 0;
@@ -884,14 +906,14 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
       if (nb) {
         // Units: CTA 0 lays out the exclusive prefix of the items' unit counts; every CTA then
         // pulls units (item, slice) from a shared cursor.
-        if (blockIdx.x == 0) {
+        if (vblock() == 0) {
           uint32_t carry = 0;
           // Unit size: about cls.units_per_cta units per CTA over the round's CTA-level work,
           // never below cls.chunk_work probes or four probe-set sizes (each unit rebuilds its
           // probe table).
           const unsigned long long rc = *(volatile unsigned long long*)&ctl->round_cost[par];
           const int64_t target =
-              max((int64_t)cls.chunk_work, (int64_t)(rc / ((unsigned long long)cls.units_per_cta * gridDim.x)));
+              max((int64_t)cls.chunk_work, (int64_t)(rc / ((unsigned long long)cls.units_per_cta * vgrid())));
           for (uint32_t j0 = 0; j0 < nb; j0 += kPT) {
             const uint32_t j = j0 + threadIdx.x;
             uint32_t c = 0;
@@ -922,7 +944,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
             ctl->cur_big[par] = 0;
           }
         }
-        if (!grid_barrier(ctl)) return;
+        if (!grid_barrier(ctl)) return false;
         const unsigned nu = *(volatile unsigned*)&ctl->units;
         while (true) {
           if (threadIdx.x < 32) {  // warp 0: take a unit, find its item (last prefix <= u), 32-way
@@ -981,11 +1003,11 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         } else {
           ok = tip_item_grid(G, W, ctl, par, x, S, work);
         }
-        if (!ok) return;
+        if (!ok) return false;
       }
     }
-    if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 2, blockIdx.x == 0 && threadIdx.x == 0 ? *(volatile unsigned long long*)&ctl->round_est[par] : 0);
+    if (!grid_barrier(ctl)) return false;
+    phase_mark(ctl, 2, vblock() == 0 && threadIdx.x == 0 ? *(volatile unsigned long long*)&ctl->round_est[par] : 0);
     // ---- phase U: touched items move to bucket max(count, k) (all unpeeled items are above
     // k here); those entering the window join the near list and feed the next minimum.
     {
@@ -1016,7 +1038,7 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         const uint32_t x = q < ns ? W.fsmall[par][q] : (q < ns + nb ? W.fbig[par][q - ns] : W.fhuge[par][q - ns - nb]);
         W.state[x] = PEELED;
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (vblock() == 0 && threadIdx.x == 0) {
         ctl->alive -= ns + nb + nh;
         ctl->rounds += 1;
         ctl->touched_total += nt;
@@ -1025,13 +1047,30 @@ __global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Work W, Ctl* ctl, Cl
         ctl->n_huge += nh;
       }
     }
-    if (!grid_barrier(ctl)) return;
+    if (!grid_barrier(ctl)) return false;
     phase_mark(ctl, 3);
   }
   unsigned long long w = work;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
   if (lane == 0 && w) atomicAdd(&ctl->work, w);
+  return true;
+}
+
+template <bool kWing>
+__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Instances I, Ctl* ctls, Classify cls) {
+  __shared__ Work sW;
+  const unsigned ib = I.n > 1 ? I.cta_beg[blockIdx.x] : 0u, ie = I.n > 1 ? I.cta_end[blockIdx.x] : 1u;
+  for (unsigned inst = ib; inst < ie; ++inst) {
+    if (threadIdx.x == 0) {
+      s_vb = I.n > 1 ? blockIdx.x - I.first[inst] : blockIdx.x;
+      s_vg = I.n > 1 ? I.ncta[inst] : gridDim.x;
+      sW = I.W[inst];
+    }
+    __syncthreads();
+    if (!peel_instance<kWing>(G, sW, ctls + inst, cls)) return;
+    __syncthreads();
+  }
 }
 
 // ---- set-up kernels -------------------------------------------------------------------------
@@ -1180,9 +1219,24 @@ void compact_side(LiveSide& L, const uint32_t* off, const uint32_t* nbr, const u
   L.cur = nx;
 }
 
+// {error bits OR-ed, unpeeled items summed} over the control blocks of one launch.
+__global__ void ctl_status_kernel(const Ctl* __restrict__ ctls, unsigned n, unsigned* out) {
+  unsigned err = 0, alive = 0;
+  for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
+    err |= ctls[i].err;
+    alive += ctls[i].alive;
+  }
+  err = __reduce_or_sync(0xffffffffu, err);
+  alive = __reduce_add_sync(0xffffffffu, alive);
+  if (threadIdx.x == 0) {
+    out[0] = err;
+    out[1] = alive;
+  }
+}
+
 template <bool kWing>
 PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t* out, cudaStream_t s,
-                    const PeelTuning& tune) {
+                    const PeelTuning& tune, const PeelParts* parts) {
   PeelResult res;
   Lists G{};
   const uint32_t* offK0 = use_v ? g.offU.get() : g.offV.get();
@@ -1202,7 +1256,25 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   DevBuf<int64_t> cnt(N, s), wk, Sx;
   DevBuf<uint32_t> eti, iota, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
   DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), fh0(N, s), fh1(N, s), tl0(N, s), tl1(N, s);
-  DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + 1, s);
+  // Independent instances (the graphs of a batch) or the whole input as one.
+  std::vector<int64_t> pbase{0}, psize{N};
+  std::vector<double> pweight{1.0};
+  if (parts && parts->base.size() > 1) {
+    PB_REQUIRE(!kWing, PB_EUNSUPPORTED, "per-graph peel instances are built for tip peeling");
+    pbase.clear();
+    psize.clear();
+    pweight.clear();
+    for (size_t i = 0; i < parts->base.size(); ++i) {
+      if (parts->size[i] <= 0) continue;
+      pbase.push_back(parts->base[i]);
+      psize.push_back(parts->size[i]);
+      pweight.push_back(std::max(parts->weight[i], 1.0));
+    }
+    if (pbase.empty()) return res;
+  }
+  const int ninst = (int)pbase.size();
+  const bool multi = ninst > 1;
+  DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + ninst, s);
   DevBuf<uint32_t> gshared(std::max(G.nK, G.nC) + 1, s);
   PB_CUDA_TRY(cudaMemsetAsync(gshared.get(), 0, gshared.bytes(), s));
   DevBuf<uint8_t> state(N, s), in_near(N, s);
@@ -1288,6 +1360,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   W.gscratch = gscratch.get();
   W.gscratch_len = scratch_len;
   W.N = N;
+  W.item0 = 0;
 
   Ctl hctl;
   std::memset(&hctl, 0, sizeof(hctl));
@@ -1299,9 +1372,9 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.alive_at_compact = (unsigned)N;
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
   // A recorded / captured pipeline runs the peel as one launch without list compaction (the
-  // host cannot step in between launches of a CUDA graph).
+  // host cannot step in between launches of a CUDA graph); so do per-graph instances.
   const bool graph_mode = g_recorder != nullptr;
-  if (graph_mode) hctl.min_gain = 0xFFFFFFFFu;
+  if (graph_mode || multi) hctl.min_gain = 0xFFFFFFFFu;
   hctl.barrier_timeout_ns = kBarrierTimeoutNs;
   hctl.near_min = (unsigned)tune.near_min;
   hctl.near_div = (unsigned)tune.near_div;
@@ -1313,35 +1386,194 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
   if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
-  DevBuf<Ctl> ctl(1, s);
-  if (capturing()) {
-    // The graph copies from host memory that outlives it; the status words come back to a
-    // pinned buffer the caller checks after every replay.
-    Ctl* h0 = (Ctl*)g_recorder->pinned_alloc(sizeof(Ctl));
-    std::memcpy(h0, &hctl, sizeof(Ctl));
-    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), h0, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-  } else {
-    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-  }
   Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
   if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
+  DevBuf<unsigned> status(2, s);
+  if (multi) {
+    // CTA shares in proportion to the instances' weights (estimated work): an instance whose
+    // share is at least one CTA gets round(share) CTAs of its own; the light ones are packed,
+    // longest first onto the least-loaded CTA, into the CTAs left over, where they run one
+    // after another.  Each instance keeps its own control block, lists and rounds, so every
+    // graph advances at its own minimum bucket.
+    std::vector<int> ord(ninst);
+    for (int i = 0; i < ninst; ++i) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return pweight[a] > pweight[b]; });
+    double wsum = 0;
+    for (double w : pweight) wsum += w;
+    int nheavy = 0;
+    while (nheavy < ninst && pweight[ord[nheavy]] / wsum * grid >= 1.0) ++nheavy;
+    double lw = 0;
+    for (int j = nheavy; j < ninst; ++j) lw += pweight[ord[j]];
+    int light_ctas = 0;
+    if (nheavy < ninst)
+      light_ctas = std::min(ninst - nheavy, std::max(1, (int)std::ceil(lw / wsum * grid)));
+    // Heavy instances share the rest; demote the lightest ones while they outnumber it.
+    while (nheavy > grid - light_ctas) {
+      --nheavy;
+      if (!light_ctas) light_ctas = 1;
+    }
+    if (!nheavy) light_ctas = std::min(grid, ninst);
+    const int hbudget = grid - light_ctas;
+    std::vector<int> ncta(ninst, 0);
+    if (nheavy) {
+      double hw = 0;
+      for (int j = 0; j < nheavy; ++j) hw += pweight[ord[j]];
+      int total = 0;
+      for (int j = 0; j < nheavy; ++j) {
+        ncta[ord[j]] = std::max(1, (int)(pweight[ord[j]] / hw * hbudget));
+        total += ncta[ord[j]];
+      }
+      for (int j = 0; total < hbudget; j = (j + 1) % nheavy, ++total) ++ncta[ord[j]];
+      while (total > hbudget) {  // some instance has more than one CTA here (hbudget >= nheavy)
+        int k = ord[0];
+        for (int j = 1; j < nheavy; ++j)
+          if (ncta[ord[j]] > ncta[k]) k = ord[j];
+        --ncta[k];
+        --total;
+      }
+    }
+    const int nlight = ninst - nheavy;
+    // Instance order of the launch: heavy ones (own CTA ranges), then each light CTA's list.
+    std::vector<int> inst_of;           // launch slot -> instance
+    std::vector<uint32_t> first, cnt, cbeg(grid, 0), cend(grid, 0);
+    uint32_t cta = 0;
+    for (int j = 0; j < nheavy; ++j) {
+      const int i = ord[j];
+      for (int c = 0; c < ncta[i]; ++c) {
+        cbeg[cta + c] = (uint32_t)inst_of.size();
+        cend[cta + c] = (uint32_t)inst_of.size() + 1;
+      }
+      inst_of.push_back(i);
+      first.push_back(cta);
+      cnt.push_back((uint32_t)ncta[i]);
+      cta += (uint32_t)ncta[i];
+    }
+    if (nlight) {
+      std::vector<std::vector<int>> bins(light_ctas);
+      std::vector<double> load(light_ctas, 0.0);
+      for (int j = nheavy; j < ninst; ++j) {
+        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        bins[b].push_back(ord[j]);
+        load[b] += pweight[ord[j]];
+      }
+      for (int b = 0; b < light_ctas; ++b, ++cta) {
+        cbeg[cta] = (uint32_t)inst_of.size();
+        for (int i : bins[b]) {
+          inst_of.push_back(i);
+          first.push_back(cta);
+          cnt.push_back(1u);
+        }
+        cend[cta] = (uint32_t)inst_of.size();
+      }
+    }
+    const int n_slots = (int)inst_of.size();
+    std::vector<Work> ws(n_slots, W);
+    std::vector<Ctl> hctls(n_slots, hctl);
+    for (int q = 0; q < n_slots; ++q) {
+      const int i = inst_of[q];
+      const int64_t b = pbase[i], n = psize[i];
+      Work& x = ws[q];
+      x.alist[0] = alist0.get() + b;
+      x.alist[1] = alist1.get() + b;
+      x.near = nearl.get() + b;
+      x.fsmall[0] = fs0.get() + b;
+      x.fsmall[1] = fs1.get() + b;
+      x.fbig[0] = fb0.get() + b;
+      x.fbig[1] = fb1.get() + b;
+      x.fchunks[0] = fc0.get() + b;
+      x.fchunks[1] = fc1.get() + b;
+      x.uprefix = upre.get() + b + i;
+      x.fhuge[0] = fh0.get() + b;
+      x.fhuge[1] = fh1.get() + b;
+      x.tlist[0] = tl0.get() + b;
+      x.tlist[1] = tl1.get() + b;
+      x.N = n;
+      x.item0 = (uint32_t)b;
+      Ctl& c = hctls[q];
+      c.alive = (unsigned)n;
+      c.alen[0] = (unsigned)n;
+      c.alive_at_compact = (unsigned)n;
+    }
+    DevBuf<Ctl> ctls(n_slots, s);
+    DevBuf<Work> dws(n_slots, s);
+    DevBuf<uint32_t> meta(2 * (size_t)n_slots + 2 * (size_t)grid, s);
+    std::vector<uint32_t> hmeta;
+    hmeta.insert(hmeta.end(), first.begin(), first.end());
+    hmeta.insert(hmeta.end(), cnt.begin(), cnt.end());
+    hmeta.insert(hmeta.end(), cbeg.begin(), cbeg.end());
+    hmeta.insert(hmeta.end(), cend.begin(), cend.end());
+    const void* src_c = hctls.data();
+    const void* src_w = ws.data();
+    const void* src_m = hmeta.data();
+    if (capturing()) {  // the graph copies from host memory that outlives it
+      void* pc = g_recorder->pinned_alloc(sizeof(Ctl) * n_slots);
+      void* pw = g_recorder->pinned_alloc(sizeof(Work) * n_slots);
+      void* pm = g_recorder->pinned_alloc(sizeof(uint32_t) * hmeta.size());
+      std::memcpy(pc, src_c, sizeof(Ctl) * n_slots);
+      std::memcpy(pw, src_w, sizeof(Work) * n_slots);
+      std::memcpy(pm, src_m, sizeof(uint32_t) * hmeta.size());
+      src_c = pc;
+      src_w = pw;
+      src_m = pm;
+    }
+    PB_CUDA_TRY(cudaMemcpyAsync(ctls.get(), src_c, sizeof(Ctl) * n_slots, cudaMemcpyHostToDevice, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(dws.get(), src_w, sizeof(Work) * n_slots, cudaMemcpyHostToDevice, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(meta.get(), src_m, sizeof(uint32_t) * hmeta.size(), cudaMemcpyHostToDevice, s));
+    Instances I{dws.get(), meta.get(), meta.get() + n_slots, meta.get() + 2 * n_slots,
+                meta.get() + 2 * n_slots + grid, (uint32_t)n_slots};
+    Ctl* cp = ctls.get();
+    void* args[] = {&G, &I, &cp, &cls};
+    PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
+    if (g_launch_counter) ++*g_launch_counter;
+    PB_LAUNCH(ctl_status_kernel, 1, 32, 0, s, cp, (unsigned)n_slots, status.get());
+    if (capturing()) {
+      PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status, status.get(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      return res;
+    }
+    PB_CUDA_TRY(cudaMemcpyAsync(hctls.data(), cp, sizeof(Ctl) * n_slots, cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (const Ctl& c : hctls) {
+      PB_REQUIRE(!(c.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
+      PB_REQUIRE(c.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
+      PB_REQUIRE(c.alive == 0, PB_ECUDA, "peeling: an instance stopped with unpeeled items");
+      res.rounds = std::max<int64_t>(res.rounds, (int64_t)c.rounds);
+      res.work += (int64_t)c.work;
+    }
+    return res;
+  }
+  DevBuf<Work> dW(1, s);
+  DevBuf<Ctl> ctl(1, s);
+  if (capturing()) {
+    // The graph copies from host memory that outlives it; the status words come back to a
+    // pinned buffer the caller checks after every replay.
+    Ctl* h0 = (Ctl*)g_recorder->pinned_alloc(sizeof(Ctl));
+    std::memcpy(h0, &hctl, sizeof(Ctl));
+    Work* w0 = (Work*)g_recorder->pinned_alloc(sizeof(Work));
+    std::memcpy(w0, &W, sizeof(Work));
+    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), h0, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(dW.get(), w0, sizeof(Work), cudaMemcpyHostToDevice, s));
+  } else {
+    PB_CUDA_TRY(cudaMemcpyAsync(ctl.get(), &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(dW.get(), &W, sizeof(Work), cudaMemcpyHostToDevice, s));
+  }
+  Instances I1{dW.get(), nullptr, nullptr, nullptr, nullptr, 1u};
   Ctl* ctl_ptr = ctl.get();
   int launches = 0;
   if (capturing()) {
-    void* args[] = {&G, &W, &ctl_ptr, &cls};
+    void* args[] = {&G, &I1, &ctl_ptr, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
     if (g_launch_counter) ++*g_launch_counter;
     // {err, alive} of the control block into the recorder's status slot (pinned).
-    PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status, &ctl_ptr->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status + 1, &ctl_ptr->alive, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    PB_LAUNCH(ctl_status_kernel, 1, 32, 0, s, ctl_ptr, 1u, status.get());
+    PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status, status.get(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     return res;
   }
   while (true) {
-    void* args[] = {&G, &W, &ctl_ptr, &cls};
+    void* args[] = {&G, &I1, &ctl_ptr, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
     if (g_launch_counter) ++*g_launch_counter;
     ++launches;
@@ -1393,13 +1625,13 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
 }  // namespace
 
 PeelResult peel_vertices(const pb_graph& g, int use_v, const int64_t* counts_dev, int64_t* tip_dev, cudaStream_t s,
-                         const PeelTuning& tune) {
-  return run_peel<false>(g, use_v, counts_dev, tip_dev, s, tune);
+                         const PeelTuning& tune, const PeelParts* parts) {
+  return run_peel<false>(g, use_v, counts_dev, tip_dev, s, tune, parts);
 }
 
 PeelResult peel_edges(const pb_graph& g, int use_v, const int64_t* ecounts_dev, int64_t* wing_dev, cudaStream_t s,
                       const PeelTuning& tune) {
-  return run_peel<true>(g, use_v, ecounts_dev, wing_dev, s, tune);
+  return run_peel<true>(g, use_v, ecounts_dev, wing_dev, s, tune, nullptr);
 }
 
 }  // namespace pb

@@ -36,6 +36,7 @@ __global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, uns
   }
 }
 
+constexpr float kPeelMargin = 0.2016f;  // log2(1.15)
 constexpr int64_t kSmall[3] = {128, 256, 512};
 constexpr int64_t kUnits[3] = {2, 4, 8};
 constexpr int64_t kChunk[3] = {512, 256, 2048};
@@ -109,6 +110,11 @@ void peel_row(const float* call_f, bool wing, int c, float* row) {
 
 int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {
   const int nc = peel_candidates(wing);
+  // Calls unlike the training data (a call feature more than 4 standard deviations from the
+  // training mean) keep the plain setting: the model has no basis to predict them.
+  bool in_range = true;
+  for (int k = 0; k < kPeelCallFeatures; ++k)
+    if (model.x_scale[k] > 0.f && std::fabs((call_f[k] - model.x_mean[k]) * model.x_scale[k]) > 4.f) in_range = false;
   std::vector<float> X((size_t)nc * kMlpIn), y(nc);
   for (int c = 0; c < nc; ++c) peel_row(call_f, wing, c, X.data() + (size_t)c * kMlpIn);
   DevBuf<float> Xd(X.size(), s), yd(nc, s);
@@ -119,6 +125,8 @@ int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log
   int best = 0;
   for (int c = 1; c < nc; ++c)
     if (y[c] < y[best]) best = c;
+  // Another setting replaces the plain one only when predicted at least 15% faster.
+  if (!in_range || y[0] - y[best] < kPeelMargin) best = 0;
   if (pred_log2ms) *pred_log2ms = y[best];
   return best;
 }

@@ -89,3 +89,18 @@ def test_batch_graph_rejects_materialising_aggregators(ctx):
     with pytest.raises(pb._ffi.PBError) as ei:
         pb.BatchGraph(dgs, "SORT", "ADEG")
     assert ei.value.status == pb._ffi.PB_EUNSUPPORTED
+
+
+def test_batch_more_graphs_than_ctas_share_them(ctx):
+    """More graphs than resident CTAs: light graphs run one after another on shared CTAs, the
+    heavy one on a CTA range of its own; every graph keeps its own peel rounds."""
+    gs = [BipartiteGraph.uniform(20 + k % 17, 15 + k % 11, 60 + k % 40, 5000 + k) for k in range(400)]
+    gs.append(BipartiteGraph.rmat(12, 11, 40000, 0.55, 0.15, 0.15, 0.15, 5400))
+    dgs = [ctx.upload(g) for g in gs]
+    counts = pb.count_batch(dgs, "BATCHS", "ADEG")
+    tips = pb.peel_batch(dgs, counts)
+    for g, c, t in zip(gs, counts, tips):
+        use_v = oracle.cmp_wedge_counts(g)[0]
+        oc, _ = oracle.count(g, "VERT", "ADEG", use_v=use_v)
+        np.testing.assert_array_equal(c, oc)
+        np.testing.assert_array_equal(t, oracle.peel_vert(g, oc, use_v=use_v)[0])
