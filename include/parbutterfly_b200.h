@@ -140,6 +140,13 @@ int64_t pb_kernel_launches(const pb_ctx* ctx);
 pb_status pb_graph_upload(pb_ctx* ctx, const pb_csr* host, pb_graph** out);
 /* Same contract, for arrays already resident in device memory (copied, not adopted). */
 pb_status pb_graph_from_device(pb_ctx* ctx, const pb_csr* dev, pb_graph** out);
+/* readBipartite (butterfly_utils.h:1008-1058) on the device: the AdjacencyHypergraph text of
+ * `len` bytes at `text` (host or device memory) is tokenised and parsed by GPU threads, its sizes
+ * and token count checked as readBipartite does (PB_EIO instead of abort), ids range-checked and
+ * the CSR validated (sorted lists) on the device. */
+pb_status pb_graph_parse_text(pb_ctx* ctx, const char* text, size_t len, pb_graph** out);
+/* The same for a file: read into pinned host memory, parsed on the device. */
+pb_status pb_graph_read_text(pb_ctx* ctx, const char* path, pb_graph** out);
 pb_status pb_graph_destroy(pb_graph* g);
 pb_status pb_graph_dims(const pb_graph* g, int64_t* nv, int64_t* nu, int64_t* m);
 
@@ -189,10 +196,10 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
  *     aggregation mode of every endpoint the block aggregator takes, among the shared-memory
  *     modes that can hold its table (dense window, hash table, dense window + hash table); the
  *     global-scratch mode remains the fallback of endpoints none of them can hold;
- *   peeling (opts.sched = PB_SCHED_LEARNED): the work-unit setting of the persistent peel kernel
- *     (which items run on a warp, how a round's CTA work is cut into units, which items take the
- *     whole grid) from a grid of PB_SCHED_WING_CANDIDATES (wing) or PB_SCHED_TIP_CANDIDATES
- *     (tip) settings (0 = the plain setting).
+ *   peeling (opts.sched = PB_SCHED_LEARNED): the setting of the persistent peel kernel — how
+ *     many CTAs it runs on, how a round's CTA work is cut into units (wing), which items run on
+ *     a warp and which take the whole grid (tip) — from a grid of PB_SCHED_WING_CANDIDATES (wing)
+ *     or PB_SCHED_TIP_CANDIDATES (tip) settings (0 = the plain setting).
  * Results are identical to the plain path's (every choice is exact).  Without an attached,
  * trained model a LEARNED call runs the plain path (stats.sched_used = 0).
  * The model learns from traces the plain path logs: with tracing on, every count call appends
@@ -202,8 +209,8 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
  * sweep the setting grid cyclically (tip and wing calls each from setting seed mod
  * the kind's number of candidates, one step per call), so that the traces cover every choice. */
 #define PB_SCHED_FEATURES 16
-#define PB_SCHED_WING_CANDIDATES 54
-#define PB_SCHED_TIP_CANDIDATES 21
+#define PB_SCHED_WING_CANDIDATES 18
+#define PB_SCHED_TIP_CANDIDATES 32
 typedef enum { PB_SCHED_COUNT = 0, PB_SCHED_PEEL = 1 } pb_sched_target;
 typedef enum { PB_TRACE_OFF = 0, PB_TRACE_PLAIN = 1, PB_TRACE_EXPLORE = 2 } pb_trace_mode;
 typedef struct pb_sched_model pb_sched_model;
@@ -271,6 +278,10 @@ void pb_csr_free(pb_csr_owned* g);
 pb_status pb_read_adjacency_hypergraph(const char* path, pb_csr_owned* out);
 /* Writer for the same format (utils/graphIO.h:752-779 layout). */
 pb_status pb_write_adjacency_hypergraph(const char* path, const pb_csr* g);
+/* The binary variant written by utils/hyperAdjToBinary.C: <base>.config ("nv mv nh mh") and
+ * <base>.vidx / .vadj / .hidx / .hadj (32-bit offsets without the final m, 32-bit ids). */
+pb_status pb_read_binary_hypergraph(const char* base, pb_csr_owned* out);
+pb_status pb_write_binary_hypergraph(const char* base, const pb_csr* g);
 /* Host validation of a CSR (same checks as pb_graph_upload). */
 pb_status pb_csr_validate(const pb_csr* g, char* msg, size_t msg_len);
 

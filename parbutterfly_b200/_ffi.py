@@ -28,12 +28,13 @@ EXPORTS = [
     "pb_count_vert_batch", "pb_peel_vert_batch", "pb_sched_model_create", "pb_sched_model_destroy",
     "pb_sched_train", "pb_sched_predict", "pb_sched_save", "pb_sched_load", "pb_ctx_set_sched_model",
     "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16", "pb_batch_create", "pb_batch_run",
-    "pb_batch_destroy",
+    "pb_batch_destroy", "pb_graph_parse_text", "pb_graph_read_text", "pb_read_binary_hypergraph",
+    "pb_write_binary_hypergraph",
 ]
 
 SCHED_FEATURES = 16
-SCHED_WING_CANDIDATES = 54
-SCHED_TIP_CANDIDATES = 21
+SCHED_WING_CANDIDATES = 18
+SCHED_TIP_CANDIDATES = 32
 SCHED_COUNT, SCHED_PEEL = 0, 1
 TRACE_OFF, TRACE_PLAIN, TRACE_EXPLORE = 0, 1, 2
 
@@ -137,6 +138,10 @@ def lib():
         "pb_batch_create": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
         "pb_batch_run": (S, [P, P, C.POINTER(P), C.POINTER(P)]),
         "pb_batch_destroy": (S, [P]),
+        "pb_graph_parse_text": (S, [P, P, C.c_size_t, C.POINTER(P)]),
+        "pb_graph_read_text": (S, [P, C.c_char_p, C.POINTER(P)]),
+        "pb_read_binary_hypergraph": (S, [C.c_char_p, C.POINTER(CSR)]),
+        "pb_write_binary_hypergraph": (S, [C.c_char_p, C.POINTER(CSR)]),
     }
     for name, (res, args) in sig.items():
         try:

@@ -120,6 +120,15 @@ class DeviceGraph:
             ctx.check(lib.pb_graph_from_device(ctx.handle, C.byref(s), C.byref(self._h)), "pb_graph_from_device")
             self.nv, self.nu, self.m = nv, nu, m
 
+    @classmethod
+    def _adopt(cls, ctx: Context, handle) -> "DeviceGraph":
+        dg = cls.__new__(cls)
+        dg.ctx, dg._h = ctx, handle
+        nv, nu, m = C.c_int64(), C.c_int64(), C.c_int64()
+        ctx.check(ctx._lib.pb_graph_dims(handle, C.byref(nv), C.byref(nu), C.byref(m)), "pb_graph_dims")
+        dg.nv, dg.nu, dg.m = nv.value, nu.value, m.value
+        return dg
+
     def close(self):
         if self._h:
             self.ctx._lib.pb_graph_destroy(self._h)
@@ -134,6 +143,28 @@ class DeviceGraph:
     @property
     def handle(self):
         return self._h
+
+
+def graph_from_text(ctx: Context, data) -> DeviceGraph:
+    """readBipartite on the device: `data` is the AdjacencyHypergraph text as bytes (host) or a
+    torch uint8 CUDA tensor; tokenised, parsed and validated by GPU kernels."""
+    h = C.c_void_p()
+    if isinstance(data, (bytes, bytearray)):
+        buf = C.create_string_buffer(bytes(data), len(data))
+        ctx.check(ctx._lib.pb_graph_parse_text(ctx.handle, buf, len(data), C.byref(h)), "pb_graph_parse_text")
+    else:
+        import torch
+        torch.cuda.synchronize()
+        ctx.check(ctx._lib.pb_graph_parse_text(ctx.handle, data.data_ptr(), data.numel(), C.byref(h)),
+                  "pb_graph_parse_text")
+    return DeviceGraph._adopt(ctx, h)
+
+
+def read_text_device(ctx: Context, path: str) -> DeviceGraph:
+    """An AdjacencyHypergraph file read into pinned memory and parsed on the device."""
+    h = C.c_void_p()
+    ctx.check(ctx._lib.pb_graph_read_text(ctx.handle, path.encode(), C.byref(h)), "pb_graph_read_text")
+    return DeviceGraph._adopt(ctx, h)
 
 
 def _ptr(a):

@@ -5,7 +5,7 @@
 //   -countType/-t, -rankType/-w, -peelType/-tp (+ -nopeel), -per/-e/-total, -m, -a, -d,
 //   -sparseType/-s, -r; Compute() at :75-277 and parallel_main() at :283-355.  Timer lines use
 //   the reference's "<name> : <seconds>" format (ligra/gettime.h:87-96, setprecision(3)).
-// Additions: -sched {plain,learned}, -autotune, -device N.
+// Additions: -sched {plain,learned}, -schedModel <file>, -autotune, -device N.
 // Differences: sparsification (-sparseType EDGE/COLOR) is approximate counting, outside this
 // path; it is rejected with an error instead of being run.
 #include <chrono>
@@ -183,6 +183,24 @@ int main(int argc, char** argv) {
   pb_ctx* ctx = nullptr;
   pb_status st = pb_ctx_create(device, nullptr, &ctx);
   if (st != PB_OK) return fail(nullptr, st, "pb_ctx_create");
+  // -sched learned: the cost models of -schedModel <file> (default: the trained models that
+  // ship beside the library, ../models/sched_b200.bin relative to this binary).
+  pb_sched_model* model = nullptr;
+  if (o.sched == PB_SCHED_LEARNED) {
+    std::string path = P.str("-schedModel", "");
+    if (path.empty()) {
+      std::string self = argv[0];
+      const size_t slash = self.find_last_of('/');
+      path = (slash == std::string::npos ? std::string(".") : self.substr(0, slash)) + "/../models/sched_b200.bin";
+    }
+    if (pb_sched_model_create(ctx, 1, &model) != PB_OK || pb_sched_load(ctx, model, path.c_str()) != PB_OK ||
+        pb_ctx_set_sched_model(ctx, model) != PB_OK) {
+      std::cerr << "no scheduler model at " << path << " (" << pb_last_error(ctx) << "); running the plain path"
+                << std::endl;
+      if (model) pb_sched_model_destroy(model);
+      model = nullptr;
+    }
+  }
 
   for (long r = 0; r < rounds + 1; ++r) {  // parallel_main re-reads the file each round (:331-341)
     pb_csr_owned h;
@@ -247,6 +265,7 @@ int main(int argc, char** argv) {
     pb_graph_destroy(g);
     pb_csr_free(&h);
   }
+  if (model) pb_sched_model_destroy(model);
   pb_ctx_destroy(ctx);
   return 0;
 }

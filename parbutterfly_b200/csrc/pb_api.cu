@@ -439,7 +439,7 @@ PeelTuning peel_setting(pb_ctx* ctx, const pb_graph& g, int use_v, bool wing, co
   row.assign(kMlpIn, 0.f);
   peel_row(f, wing, c, row.data());
   st.ms_sched = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  return peel_candidate(wing, c);
+  return peel_candidate(wing, c, 2 * sm_count());
 }
 
 void log_peel_trace(pb_ctx* ctx, const std::vector<float>& row, double ms) {
@@ -605,6 +605,45 @@ pb_status pb_graph_upload(pb_ctx* ctx, const pb_csr* host, pb_graph** out) {
 
 pb_status pb_graph_from_device(pb_ctx* ctx, const pb_csr* dev, pb_graph** out) {
   return guarded(ctx, [&] { upload_graph(ctx, dev, true, out); });
+}
+
+pb_status pb_graph_parse_text(pb_ctx* ctx, const char* text, size_t len, pb_graph** out) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(text && out, PB_EINVAL, "null argument");
+    ParsedCSR P;
+    parse_adjacency_hypergraph(text, len, is_device_ptr(text), P, ctx->stream);
+    const pb_csr c{P.nv, P.nu, P.m, P.offV.get(), P.edgV.get(), P.offU.get(), P.edgU.get()};
+    upload_graph(ctx, &c, true, out);  // validated on the device (offsets, ranges, sorted lists)
+  });
+}
+
+pb_status pb_graph_read_text(pb_ctx* ctx, const char* path, pb_graph** out) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(path && out, PB_EINVAL, "null argument");
+    FILE* f = fopen(path, "rb");
+    PB_REQUIRE(f, PB_EIO, std::string("cannot open ") + path);
+    fseek(f, 0, SEEK_END);
+    const long len = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    char* buf = nullptr;
+    if (len > 0 && cudaMallocHost((void**)&buf, (size_t)len) != cudaSuccess) {
+      fclose(f);
+      throw Error{PB_ENOMEM, "pinned host allocation for the file failed"};
+    }
+    const size_t got = len > 0 ? fread(buf, 1, (size_t)len, f) : 0;
+    fclose(f);
+    try {
+      PB_REQUIRE(got == (size_t)(len > 0 ? len : 0), PB_EIO, std::string("short read of ") + path);
+      ParsedCSR P;
+      parse_adjacency_hypergraph(buf ? buf : "", (size_t)(len > 0 ? len : 0), false, P, ctx->stream);
+      const pb_csr c{P.nv, P.nu, P.m, P.offV.get(), P.edgV.get(), P.offU.get(), P.edgU.get()};
+      upload_graph(ctx, &c, true, out);
+    } catch (...) {
+      if (buf) cudaFreeHost(buf);
+      throw;
+    }
+    if (buf) cudaFreeHost(buf);
+  });
 }
 
 pb_status pb_graph_destroy(pb_graph* g) {

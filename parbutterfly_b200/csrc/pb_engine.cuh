@@ -92,6 +92,14 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
 CountResult count_ranked_materialized(const Ranked& R, int per, int64_t* out, bool hist, int64_t max_wedges,
                                       cudaStream_t s);
 
+// Device parsing of the AdjacencyHypergraph text (pb_parse.cu): the four CSR arrays of the
+// file in `text` (len bytes, host or device memory), offsets including the final m.
+struct ParsedCSR {
+  int64_t nv = 0, nu = 0, m = 0;
+  DevBuf<uint32_t> offV, edgV, offU, edgU;
+};
+void parse_adjacency_hypergraph(const char* text, size_t len, bool on_device, ParsedCSR& out, cudaStream_t s);
+
 // Batches (pb_batch.cu): the disjoint union of k graphs, each graph's count side on the union's
 // U side (count with use_v = 1); kbase/ksize locate each graph's count side in the union.
 void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int64_t>& kbase,
@@ -110,6 +118,7 @@ struct PeelTuning {
   int64_t units_per_cta = 4;              // CTA work units per CTA and round (wing)
   int64_t near_min = 32768;               // the near window holds at least this many items
   int64_t near_div = 64;                  // ... or alive / near_div
+  int64_t max_ctas = 0;                   // CTAs of the persistent kernel (0: all resident)
 };
 // The plain path's settings: wing items never take the whole grid; tip items above 2^13
 // wedges do (one CTA per heavy vertex leaves the rest of the GPU idle in most rounds).

@@ -165,4 +165,68 @@ pb_status pb_write_adjacency_hypergraph(const char* path, const pb_csr* g) {
   return std::fclose(f) == 0 ? PB_OK : PB_EIO;
 }
 
+
+// hyperAdjToBinary's output (utils/hyperAdjToBinary.C): <base>.config holds "nv mv nh mh" as
+// text; <base>.vidx / .vadj / .hidx / .hadj hold offsetsV[nv], edgesV[mv], offsetsH[nh],
+// edgesH[mh] as raw 32-bit words (uintT / uintE of the default build).
+pb_status pb_read_binary_hypergraph(const char* base, pb_csr_owned* out) {
+  if (!base || !out) return PB_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  const std::string b(base);
+  FILE* cf = std::fopen((b + ".config").c_str(), "r");
+  if (!cf) return PB_EIO;
+  unsigned long long nv = 0, mv = 0, nh = 0, mh = 0;
+  const int got = std::fscanf(cf, "%llu %llu %llu %llu", &nv, &mv, &nh, &mh);
+  std::fclose(cf);
+  if (got != 4 || mv != mh) return PB_EIO;
+  if (nv + nh >= (1ull << 31) || 2 * mv > 0xFFFFFFFFull) return PB_ETOOBIG;
+  auto read_words = [&](const char* ext, uint32_t* dst, unsigned long long n) -> bool {
+    FILE* f = std::fopen((b + ext).c_str(), "rb");
+    if (!f) return false;
+    const size_t r = n ? std::fread(dst, sizeof(uint32_t), (size_t)n, f) : 0;
+    std::fclose(f);
+    return r == (size_t)n;
+  };
+  out->nv = (int64_t)nv;
+  out->nu = (int64_t)nh;
+  out->m = (int64_t)mv;
+  out->offsetsV = (uint32_t*)std::malloc(sizeof(uint32_t) * (nv + 1));
+  out->offsetsU = (uint32_t*)std::malloc(sizeof(uint32_t) * (nh + 1));
+  out->edgesV = (uint32_t*)std::malloc(sizeof(uint32_t) * (mv ? mv : 1));
+  out->edgesU = (uint32_t*)std::malloc(sizeof(uint32_t) * (mv ? mv : 1));
+  if (!out->offsetsV || !out->offsetsU || !out->edgesV || !out->edgesU) {
+    pb_csr_free(out);
+    return PB_ENOMEM;
+  }
+  if (!read_words(".vidx", out->offsetsV, nv) || !read_words(".vadj", out->edgesV, mv) ||
+      !read_words(".hidx", out->offsetsU, nh) || !read_words(".hadj", out->edgesU, mv)) {
+    pb_csr_free(out);
+    return PB_EIO;
+  }
+  out->offsetsV[nv] = (uint32_t)mv;
+  out->offsetsU[nh] = (uint32_t)mv;
+  return PB_OK;
+}
+
+// Writes the same five files.
+pb_status pb_write_binary_hypergraph(const char* base, const pb_csr* g) {
+  if (!base || !g) return PB_EINVAL;
+  const std::string b(base);
+  FILE* cf = std::fopen((b + ".config").c_str(), "w");
+  if (!cf) return PB_EIO;
+  std::fprintf(cf, "%lld %lld %lld %lld", (long long)g->nv, (long long)g->m, (long long)g->nu, (long long)g->m);
+  std::fclose(cf);
+  auto write_words = [&](const char* ext, const uint32_t* src, int64_t n) -> bool {
+    FILE* f = std::fopen((b + ext).c_str(), "wb");
+    if (!f) return false;
+    const size_t w = n ? std::fwrite(src, sizeof(uint32_t), (size_t)n, f) : 0;
+    std::fclose(f);
+    return w == (size_t)n;
+  };
+  if (!write_words(".vidx", g->offsetsV, g->nv) || !write_words(".vadj", g->edgesV, g->m) ||
+      !write_words(".hidx", g->offsetsU, g->nu) || !write_words(".hadj", g->edgesU, g->m))
+    return PB_EIO;
+  return PB_OK;
+}
+
 }  // extern "C"

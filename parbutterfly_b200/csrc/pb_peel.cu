@@ -1329,7 +1329,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   int per_sm = 0;
   PB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
   PB_REQUIRE(per_sm >= 1, PB_ECUDA, "peeling kernel does not fit on an SM");
-  const int grid = sm_count() * per_sm;
+  int grid = sm_count() * per_sm;
+  // A single instance may run on fewer CTAs: its barriers and grid-stride phases then span
+  // fewer CTAs, which shortens light rounds.
+  int64_t cap = parts && parts->base.size() > 1 ? 0 : tune.max_ctas;
+  if (const char* e = getenv("PB_PEEL_CTAS")) cap = atoll(e);  // diagnostic hook
+  if (cap > 0) grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, cap));
 
   DevBuf<uint32_t> gscratch;
   if (need_scratch) {

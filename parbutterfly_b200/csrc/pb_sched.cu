@@ -37,33 +37,31 @@ __global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, uns
 }
 
 constexpr float kPeelMargin = 0.2016f;  // log2(1.15)
-constexpr int64_t kSmall[3] = {128, 256, 512};
-constexpr int64_t kUnits[3] = {2, 4, 8};
-constexpr int64_t kChunk[3] = {512, 256, 2048};
-constexpr int64_t kWingHuge[2] = {int64_t(1) << 40, int64_t(1) << 22};
-constexpr int64_t kTipHuge[7] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) << 12, int64_t(1) << 14,
-                                 int64_t(1) << 15, int64_t(1) << 16, int64_t(1) << 40};
+constexpr int64_t kUnits[3] = {4, 2, 8};
+constexpr int64_t kChunk[2] = {512, 2048};
+constexpr int64_t kTipSmall[2] = {512, 256};
+constexpr int64_t kTipHuge[4] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) << 15, int64_t(1) << 40};
+constexpr int kCtaDiv[4] = {1, 2, 4, 8};
 
 }  // namespace
 
 int peel_candidates(bool wing) { return wing ? kWingCandidates : kTipCandidates; }
 
-PeelTuning peel_candidate(bool wing, int c) {
+PeelTuning peel_candidate(bool wing, int c, int resident_ctas) {
   PeelTuning t = plain_peel_tuning(wing);
+  int div = 1;
   if (wing) {
-    // c = ((small * 3 + units) * 3 + chunk) * 2 + huge, ordered so that c = 0 is the plain
-    // setting (small 512, units 4, chunk 512, huge never).
-    const int h = c % 2, ch = (c / 2) % 3, un = (c / 6) % 3, sm = (c / 18) % 3;
-    t.small_work = kSmall[(sm + 2) % 3];
-    t.units_per_cta = kUnits[(un + 1) % 3];
-    t.chunk_work = kChunk[ch];
-    t.huge_work = kWingHuge[h];
+    // c = (units * 2 + chunk) * 3 + cta divisor; c = 0 is the plain setting.
+    div = kCtaDiv[c % 3];
+    t.chunk_work = kChunk[(c / 3) % 2];
+    t.units_per_cta = kUnits[(c / 6) % 3];
   } else {
-    // c = small * 7 + huge; c = 0 is the plain setting (small 512, huge 2^13).
-    const int h = c % 7, sm = (c / 7) % 3;
-    t.small_work = kSmall[(sm + 2) % 3];
-    t.huge_work = kTipHuge[h];
+    // c = (small * 4 + huge) * 4 + cta divisor; c = 0 is the plain setting.
+    div = kCtaDiv[c % 4];
+    t.huge_work = kTipHuge[(c / 4) % 4];
+    t.small_work = kTipSmall[(c / 16) % 2];
   }
+  t.max_ctas = div > 1 ? std::max(1, resident_ctas / div) : 0;
   return t;
 }
 
@@ -100,12 +98,12 @@ void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* 
 }
 
 void peel_row(const float* call_f, bool wing, int c, float* row) {
-  const PeelTuning t = peel_candidate(wing, c);
+  const PeelTuning t = peel_candidate(wing, c, 1 << 20);
   for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
   row[12] = (float)std::log2((double)t.small_work);
-  row[13] = (float)std::log2((double)t.units_per_cta);
-  row[14] = (float)std::log2((double)t.chunk_work);
-  row[15] = t.huge_work < (int64_t(1) << 40) ? (float)std::log2((double)t.huge_work) : 0.f;
+  row[13] = wing ? (float)std::log2((double)t.units_per_cta) : (float)std::log2((double)std::min<int64_t>(t.huge_work, int64_t(1) << 20));
+  row[14] = wing ? (float)std::log2((double)t.chunk_work) : 0.f;
+  row[15] = t.max_ctas > 0 ? (float)std::log2((double)((1 << 20) / t.max_ctas)) : 0.f;  // log2 of the CTA divisor
 }
 
 int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {

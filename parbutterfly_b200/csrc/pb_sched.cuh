@@ -7,12 +7,13 @@
 namespace pb {
 
 constexpr int kPeelCallFeatures = 12;  // call-level features; 4 candidate slots follow
-constexpr int kWingCandidates = 54;    // 3 small x 3 units x 3 chunk x 2 grid-level settings
-constexpr int kTipCandidates = 21;     // 3 small x 7 grid-level settings
+constexpr int kWingCandidates = 18;    // 3 units x 2 chunk x 3 CTA counts
+constexpr int kTipCandidates = 32;     // 2 small x 4 grid-level thresholds x 4 CTA counts
 
 int peel_candidates(bool wing);
-// Work-unit setting c of the candidate grid of a peel kind (c = 0: the plain path's setting).
-PeelTuning peel_candidate(bool wing, int c);
+// Work-unit setting c of the candidate grid of a peel kind (c = 0: the plain path's setting);
+// resident_ctas is the CTA count of a full persistent launch.
+PeelTuning peel_candidate(bool wing, int c, int resident_ctas);
 // Call-level features of a peel call (kPeelCallFeatures floats into f).
 void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* counts_dev, float* f, cudaStream_t s);
 // Cost-model row of candidate c for a call (kMlpIn floats).

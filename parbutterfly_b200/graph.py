@@ -158,6 +158,17 @@ class BipartiteGraph:
         _ffi.check(_ffi.lib().pb_read_adjacency_hypergraph(os.fsencode(path), C.byref(s)), what=path)
         return BipartiteGraph._from_owned(s)
 
+    def write_binary(self, base: str) -> None:
+        """hyperAdjToBinary's layout: base.config, .vidx, .vadj, .hidx, .hadj."""
+        s = self.csr_struct()
+        _ffi.check(_ffi.lib().pb_write_binary_hypergraph(os.fsencode(base), C.byref(s)), what=base)
+
+    @staticmethod
+    def read_binary(base: str) -> "BipartiteGraph":
+        s = _ffi.CSR()
+        _ffi.check(_ffi.lib().pb_read_binary_hypergraph(os.fsencode(base), C.byref(s)), what=base)
+        return BipartiteGraph._from_owned(s)
+
 
 # ---- the benchmark workloads -----------------------------------------------------------------
 def workload(name: str) -> BipartiteGraph:

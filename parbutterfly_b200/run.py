@@ -3,6 +3,8 @@
     python -m parbutterfly_b200.run count-edge --graph rmat20    # pb_count_edge(HASH, ACOCORE)
     python -m parbutterfly_b200.run peel-edge --graph rmat15     # count, then pb_peel_edge
     python -m parbutterfly_b200.run peel-vert --graph rmat20     # count, then pb_peel_vert
+    python -m parbutterfly_b200.run mlp-train                    # the cost model on the tensor cores
+    python -m parbutterfly_b200.run batch-graph                  # the 256-graph batch as a CUDA graph
 
 Graphs: rmat20 = bipartite R-MAT 2^20 x 2^18, m = 2^24, (.55,.15,.15,.15), seed 2 (the
 benchmark workload); rmat15 = the same generator at 2^15 x 2^13, m = 2^19; rmat14 at
@@ -24,12 +26,35 @@ GRAPHS = {
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["count-edge", "count-vert", "count-total", "peel-edge", "peel-vert"])
+    ap.add_argument("case", choices=["count-edge", "count-vert", "count-total", "peel-edge", "peel-vert", "mlp-train",
+                                     "batch-graph"])
     ap.add_argument("--graph", default="rmat15", choices=sorted(GRAPHS))
     ap.add_argument("--count-type", default="HASH")
     ap.add_argument("--rank-type", default="ACOCORE")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
+    if a.case == "mlp-train":
+        import numpy as np
+        rng = np.random.default_rng(0)
+        X = rng.normal(size=(65536, 16)).astype(np.float32)
+        y = (np.sin(X[:, 0]) + X[:, 1] * X[:, 2]).astype(np.float32)
+        with pb.Context(0) as ctx:
+            m = pb.SchedModel(ctx, seed=1)
+            for _ in range(a.repeat):
+                mse = m.train(m.COUNT, X, y, epochs=2, batch=8192, lr=3e-3)
+                print(f"mlp-train rows={len(y)} mse={mse:.4f}")
+            m.close()
+        return 0
+    if a.case == "batch-graph":
+        gs = [BipartiteGraph.batch_member(k) for k in range(256)]
+        with pb.Context(0) as ctx:
+            dgs = [ctx.upload(g) for g in gs]
+            bg = pb.BatchGraph(dgs, "BATCHS", "ADEG", autotune=True)
+            for _ in range(a.repeat):
+                bg.run(copy_out=False)
+                print(f"batch-graph replay ms={ctx.stats()['ms_count']:.1f}")
+            bg.close()
+        return 0
     g = GRAPHS[a.graph]()
     with pb.Context(0) as ctx:
         dg = ctx.upload(g)

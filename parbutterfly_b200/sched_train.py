@@ -37,6 +37,7 @@ PEEL_GRAPHS = [
     ("rmat", (16, 15, 1 << 19, 0.57, 0.19, 0.19, 0.05), 7103),
     ("zipf", (1 << 15, 1 << 13, 1 << 18, 1.5), 7104),
     ("uniform", (1 << 13, 1 << 12, 1 << 17), 7105),
+    ("rmat", (17, 15, 1 << 21, 0.55, 0.15, 0.15, 0.15), 7106),
 ]
 
 
@@ -48,7 +49,7 @@ def make(kind, args, seed) -> BipartiteGraph:
     return BipartiteGraph.uniform(*args, seed)
 
 
-def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=54, log=print):
+def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=32, log=print):
     """Explore-mode traces: returns (Xc, yc, Xp, yp)."""
     pb.trace_clear(ctx)
     pb.trace_set(ctx, "explore", seed=1)
@@ -96,9 +97,9 @@ def main():
     ap.add_argument("--quick", action="store_true", help="fewer graphs and peel settings")
     a = ap.parse_args()
     ctx = pb.Context(a.device)
-    cg, pg, ps = COUNT_GRAPHS, PEEL_GRAPHS, 54
+    cg, pg, ps = COUNT_GRAPHS, PEEL_GRAPHS, 32
     if a.quick:
-        cg, pg, ps = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 18
+        cg, pg, ps = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16
     Xc, yc, Xp, yp = collect(ctx, cg, pg, ps)
     m = train(ctx, Xc, yc, Xp, yp)
     m.save(a.out)

@@ -122,3 +122,17 @@ def test_context_without_gpu_reports_status():
     h = C.c_void_p()
     st = _ffi.lib().pb_ctx_create(0, None, C.byref(h))
     assert st == _ffi.PB_ECUDA and not h.value
+
+
+def test_binary_format_roundtrip(tmp_path):
+    g = BipartiteGraph.rmat(9, 8, 3000, 0.55, 0.15, 0.15, 0.15, 31)
+    base = str(tmp_path / "g")
+    g.write_binary(base)
+    cfg = open(base + ".config").read().split()
+    assert [int(x) for x in cfg] == [g.nv, g.m, g.nu, g.m]
+    assert os.path.getsize(base + ".vidx") == 4 * g.nv  # offsets without the final m
+    h = BipartiteGraph.read_binary(base)
+    for name in ("offsetsV", "edgesV", "offsetsU", "edgesU"):
+        np.testing.assert_array_equal(getattr(h, name), getattr(g, name))
+    with pytest.raises(_ffi.PBError):
+        BipartiteGraph.read_binary(str(tmp_path / "missing"))
