@@ -528,10 +528,7 @@ void MlpModel::predict_dev(const float* X_dev, int64_t n, float* y_dev, cudaStre
   const Norm nm = norm_of(*this);
   PB_LAUNCH(gather_standardize_kernel, grid_for(n * kMlpIn, 256), 256, 0, stream, X_dev, nullptr, nullptr, n, nm,
             A.Xh.get(), nullptr);
-  cudaStream_t keep = s;
-  s = stream;
   forward(*this, A, n, stream);
-  s = keep;
   PB_LAUNCH(destandardize_kernel, grid_for(n, 256), 256, 0, stream, A.Y.get(), n, y_mean, 1.f / y_scale, y_dev);
   check_err(*this, stream);
 }

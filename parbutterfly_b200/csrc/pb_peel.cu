@@ -224,6 +224,8 @@ __device__ __forceinline__ bool t_get(const uint32_t* keys, const uint32_t* vals
 
 __device__ __forceinline__ uint32_t np2(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
 
+constexpr uint32_t kLocalUnits = 2048;  // rounds with at most this many CTA-level items lay
+                                        // out their work units in every CTA's shared memory
 struct Shared {
   uint32_t incl[kPT];
   uint32_t sb[kPT];
@@ -231,6 +233,7 @@ struct Shared {
   unsigned long long red[32];
   uint32_t item;
   unsigned hist[66];
+  uint32_t uprefix[kLocalUnits + 1];
 };
 
 // Flattened two-level iteration by one warp: first(j, L, sb) gives the second-level range
@@ -904,9 +907,12 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
       __syncthreads();  // warp tables and the CTA table share memory
       const unsigned nb = *(volatile unsigned*)&ctl->flen_big[par];
       if (nb) {
-        // Units: CTA 0 lays out the exclusive prefix of the items' unit counts; every CTA then
-        // pulls units (item, slice) from a shared cursor.
-        if (vblock() == 0) {
+        // Units: the exclusive prefix of the items' unit counts; every CTA then pulls units
+        // (item, slice) from a shared cursor.  Up to kLocalUnits items every CTA computes the
+        // same prefix in its shared memory (from the costs phase F froze), so no grid barrier
+        // is needed; beyond that CTA 0 lays it out in global memory behind a barrier.
+        const bool local = nb <= kLocalUnits;
+        if (local || vblock() == 0) {
           uint32_t carry = 0;
           // Unit size: about cls.units_per_cta units per CTA over the round's CTA-level work,
           // never below cls.chunk_work probes or four probe-set sizes (each unit rebuilds its
@@ -931,21 +937,29 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
               } else {
                 c = 1;
               }
-              W.fchunks[par][j] = c;
+              if (!local) W.fchunks[par][j] = c;
             }
             uint32_t T;
             const uint32_t incl = block_incl_scan(c, S.scan, T);
-            if (j < nb) W.uprefix[j] = carry + incl - c;
+            if (j < nb) {
+              if (local) S.uprefix[j] = carry + incl - c;
+              else W.uprefix[j] = carry + incl - c;
+            }
             carry += T;
           }
           if (threadIdx.x == 0) {
-            W.uprefix[nb] = carry;
-            ctl->units = carry;
-            ctl->cur_big[par] = 0;
+            if (local) {
+              S.uprefix[nb] = carry;
+            } else {
+              W.uprefix[nb] = carry;
+              ctl->units = carry;
+            }
           }
         }
-        if (!grid_barrier(ctl)) return false;
-        const unsigned nu = *(volatile unsigned*)&ctl->units;
+        if (local) __syncthreads();
+        else if (!grid_barrier(ctl)) return false;
+        const uint32_t* upre = local ? S.uprefix : W.uprefix;
+        const unsigned nu = local ? S.uprefix[nb] : *(volatile unsigned*)&ctl->units;
         while (true) {
           if (threadIdx.x < 32) {  // warp 0: take a unit, find its item (last prefix <= u), 32-way
             unsigned u = 0;
@@ -956,7 +970,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
               while (hi - lo > 1) {
                 const uint32_t step = (hi - lo + 31) / 32;
                 const uint32_t idx = lo + lane * step;
-                const bool le = idx < hi && W.uprefix[idx] <= u;
+                const bool le = idx < hi && upre[idx] <= u;
                 const unsigned bal = __ballot_sync(0xffffffffu, le);
                 const uint32_t last = 31 - __clz(bal);  // lane 0 always qualifies (prefix[lo] <= u)
                 lo = lo + last * step;
@@ -980,7 +994,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             E.v = G.center_of[x];
             E.u = G.u_of[x];
             E.from_v = cls.wing_from_v(G, E.v, E.u);
-            const uint32_t base = W.uprefix[q], nch = W.uprefix[q + 1] - base;
+            const uint32_t base = upre[q], nch = upre[q + 1] - base;
             wing_item<LV_BLOCK>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work, u - base, nch);
           } else {
             tip_item_block(G, W, ctl, par, x, pool, S, work);

@@ -5,8 +5,8 @@ workloads (other seeds and sizes): bipartite R-MAT with three skews, Zipf-endpoi
 uniform graphs.  With tracing in explore mode the plain path logs
   - count: one row per block-aggregator item of every count call (VERT and EDGE, HASH),
     with a random valid aggregation mode per item (target log2 SM cycles of the item);
-  - peel:  one row per tip / wing peel call, sweeping the work-unit setting grid
-    (target log2 ms of the call).
+  - peel:  one row per tip / wing peel call, sweeping the setting grid (target log2 ms of the
+    call); two larger graphs are traced for tip peeling only.
 Both MLPs are then trained on the GPU (tensor-core forward / backward, Adam) and saved.
 
     python -m parbutterfly_b200.sched_train --out sched.bin [--quick]
@@ -39,6 +39,11 @@ PEEL_GRAPHS = [
     ("uniform", (1 << 13, 1 << 12, 1 << 17), 7105),
     ("rmat", (17, 15, 1 << 21, 0.55, 0.15, 0.15, 0.15), 7106),
 ]
+# Larger graphs traced for tip peeling only (a wing sweep of them would take minutes).
+TIP_GRAPHS = [
+    ("rmat", (19, 17, 1 << 23, 0.55, 0.15, 0.15, 0.15), 7201),
+    ("rmat", (18, 17, 1 << 22, 0.57, 0.19, 0.19, 0.05), 7202),
+]
 
 
 def make(kind, args, seed) -> BipartiteGraph:
@@ -49,7 +54,8 @@ def make(kind, args, seed) -> BipartiteGraph:
     return BipartiteGraph.uniform(*args, seed)
 
 
-def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=32, log=print):
+def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=32, log=print,
+            tip_graphs=TIP_GRAPHS):
     """Explore-mode traces: returns (Xc, yc, Xp, yp)."""
     pb.trace_clear(ctx)
     pb.trace_set(ctx, "explore", seed=1)
@@ -72,6 +78,14 @@ def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS,
                 pb.peel_e(dg, ce)
             dg.close()
             log(f"[sched_train] peel traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
+        for spec in tip_graphs:
+            t0 = time.perf_counter()
+            dg = ctx.upload(make(*spec))
+            c = pb.count(dg, "BATCHS", "ADEG")
+            for k in range(peel_settings):
+                pb.peel(dg, c)
+            dg.close()
+            log(f"[sched_train] tip traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
     finally:
         pb.trace_set(ctx, "off")
     Xc, yc = pb.trace_rows(ctx, pb.SchedModel.COUNT)
@@ -97,10 +111,10 @@ def main():
     ap.add_argument("--quick", action="store_true", help="fewer graphs and peel settings")
     a = ap.parse_args()
     ctx = pb.Context(a.device)
-    cg, pg, ps = COUNT_GRAPHS, PEEL_GRAPHS, 32
+    cg, pg, ps, tg = COUNT_GRAPHS, PEEL_GRAPHS, 32, TIP_GRAPHS
     if a.quick:
-        cg, pg, ps = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16
-    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps)
+        cg, pg, ps, tg = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16, []
+    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps, tip_graphs=tg)
     m = train(ctx, Xc, yc, Xp, yp)
     m.save(a.out)
     print(f"[sched_train] saved {a.out}")
