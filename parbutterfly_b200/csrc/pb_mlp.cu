@@ -319,15 +319,14 @@ void MlpModel::init(uint64_t seed, cudaStream_t stream) {
   std::vector<float> p(kParams, 0.f);
   uint64_t st = seed;
   // He-style uniform initialisation; biases zero.
-  auto fill = [&](int off, int rows, int cols, int live_rows) {
+  auto fill = [&](int off, int cols, int live_rows) {  // live_rows x cols, row-major
     const double a = std::sqrt(6.0 / cols);
     for (int r = 0; r < live_rows; ++r)
       for (int c = 0; c < cols; ++c) p[off + r * cols + c] = (float)((2.0 * uniform01(st) - 1.0) * a);
-    (void)rows;
   };
-  fill(kOffW1, kMlpHidden, kMlpIn, kMlpHidden);
-  fill(kOffW2, kMlpHidden, kMlpHidden, kMlpHidden);
-  fill(kOffW3, kMlpOutPad, kMlpHidden, 1);
+  fill(kOffW1, kMlpIn, kMlpHidden);
+  fill(kOffW2, kMlpHidden, kMlpHidden);
+  fill(kOffW3, kMlpHidden, 1);  // output layer: row 0 only
   params.alloc(kParams, s);
   grads.alloc(kParams, s);
   m_adam.alloc(kParams, s);
