@@ -68,7 +68,10 @@ struct Ctl {
   unsigned long long pbin_ns[42], pbin_rounds[42], pbin_est[42];
   // Near-window size: at least near_min items, or alive / near_div.
   unsigned near_min, near_div;
+  // Barriers of CTA groups that process heavy tip items concurrently.
+  unsigned gbar_count[32], gbar_gen[32];
 };
+constexpr unsigned kMaxGroups = 32;
 
 
 // Live adjacency of both sides.  Lists are compacted to their live entries between launches
@@ -102,7 +105,10 @@ struct Work {
   uint32_t* uprefix;     // exclusive prefix of fchunks for the current round (N + 1)
   uint32_t* fhuge[2];
   uint32_t* tlist[2];
-  uint32_t* gshared;   // grid-shared dense counters / probe markers for huge items (zeroed)
+  uint32_t* gshared;   // grid-shared dense counters / probe markers for huge items (zeroed);
+                       // tip: ngroups slices of gshared_stride counters, one per CTA group
+  int64_t gshared_stride;
+  unsigned ngroups;
   uint32_t* gscratch;  // per-CTA dense scratch (dense counters / probe markers)
   int64_t gscratch_len;
   int64_t N;           // items of this instance
@@ -173,6 +179,38 @@ __device__ bool grid_barrier(Ctl* ctl) {
   }
   __syncthreads();
   return ok != 0;
+}
+
+// Barrier over `size` CTAs of a group (slot: the group's counters).  Bounded like grid_barrier.
+__device__ bool group_barrier(Ctl* ctl, unsigned slot, unsigned size) {
+  __shared__ int gok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &ctl->gbar_gen[slot];
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&ctl->gbar_count[slot], 1u);
+    gok = 1;
+    if (arrived == size - 1) {
+      atomicExch(&ctl->gbar_count[slot], 0u);
+      __threadfence();
+      atomicAdd(&ctl->gbar_gen[slot], 1u);
+    } else {
+      const unsigned long long t0 = globaltimer_ns();
+      while (*vgen == gen) {
+        if (*(volatile unsigned*)&ctl->err) { gok = 0; break; }
+        if (globaltimer_ns() - t0 > ctl->barrier_timeout_ns) {
+          atomicOr(&ctl->err, ERR_TIMEOUT);
+          gok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    if (*(volatile unsigned*)&ctl->err) gok = 0;
+  }
+  __syncthreads();
+  return gok != 0;
 }
 
 // Fibonacci hashing: the high bits of key * 2^32/phi, folded into the table size.
@@ -657,6 +695,33 @@ __device__ bool tip_item_grid(const Lists& G, const Work& W, Ctl* ctl, unsigned 
   return grid_barrier(ctl);
 }
 
+// The same for a group of gs CTAs (this CTA is number lb in it) with its own counter slice and
+// barrier: several heavy tip items of a round run at once, one per group.  The caller's grid
+// barrier after the group's item separates it from the next use of the slice.
+__device__ bool tip_item_group(const Lists& G, const Work& W, Ctl* ctl, unsigned par, uint32_t u, Shared& S,
+                               unsigned long long& work, unsigned lb, unsigned gs, unsigned slot, uint32_t* cnt) {
+  auto first = [&](uint32_t j, uint32_t& L, uint32_t& sb) {
+    const uint32_t v = G.edgK[j];
+    sb = G.offC[v];
+    L = G.offC[v + 1] - sb;
+  };
+  const uint64_t T = (uint64_t)G.wk[u] + (G.offK[u + 1] - G.offK[u]);
+  const uint64_t lo = T * lb / gs, hi = T * (lb + 1) / gs;
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+    const uint32_t u2 = G.edgC[q];
+    if (u2 != u) atomicAdd(&cnt[u2], 1u);
+  }, lo, hi);
+  if (!group_barrier(ctl, slot, gs)) return false;
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
+    const uint32_t u2 = G.edgC[q];
+    if (u2 == u) return;
+    const int64_t w = atomicExch(&cnt[u2], 0u);
+    if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
+  }, lo, hi);
+  if (lb == 0 && threadIdx.x == 0) work += T;
+  return true;
+}
+
 // ---- the persistent kernel ------------------------------------------------------------------
 // Wing items run on one warp when their work is small and their probe set fits a warp table.
 struct Classify {
@@ -1001,9 +1066,25 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
           }
         }
       }
-      // Huge items, one at a time, each spread over every CTA of the grid.
+      // Huge items: tip items in waves of up to ngroups at once, one per CTA group (equal
+      // splits of the instance's CTAs); otherwise one at a time over every CTA.
       const unsigned nh = *(volatile unsigned*)&ctl->flen_huge[par];
-      for (unsigned q = 0; q < nh; ++q) {
+      const unsigned ng = kWing ? 1u : min(W.ngroups, vgrid());
+      if (!kWing && nh > 1 && ng > 1) {
+        const unsigned vg = vgrid(), vb = vblock();
+        for (unsigned w0 = 0; w0 < nh; w0 += ng) {
+          const unsigned gn = min(ng, nh - w0);
+          const unsigned grp = vb * gn / vg;
+          const unsigned g0 = (grp * vg + gn - 1) / gn, g1 = ((grp + 1) * vg + gn - 1) / gn;
+          const uint32_t x = W.fhuge[par][w0 + grp];
+          if (W.cnt[x] != 0 &&  // uniform across the group
+              !tip_item_group(G, W, ctl, par, x, S, work, vb - g0, g1 - g0, grp,
+                              W.gshared + (size_t)grp * (size_t)W.gshared_stride))
+            return false;
+          if (w0 + ng < nh && !grid_barrier(ctl)) return false;  // the slices are reused next wave
+        }
+      }
+      for (unsigned q = 0; q < nh && (kWing || nh == 1 || ng <= 1); ++q) {
         const uint32_t x = W.fhuge[par][q];
         if (W.cnt[x] == 0) continue;  // frontier counts do not change during the phase
         bool ok;
@@ -1289,7 +1370,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   const int ninst = (int)pbase.size();
   const bool multi = ninst > 1;
   DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + ninst, s);
-  DevBuf<uint32_t> gshared(std::max(G.nK, G.nC) + 1, s);
+  // Grid-shared dense counters: tip peeling keeps one slice per CTA group (heavy items of a round
+  // run concurrently), up to 32 slices within 256 MB.
+  const int64_t gstride = std::max(G.nK, G.nC) + 1;
+  const unsigned ngroups =
+      kWing ? 1u : (unsigned)std::max<int64_t>(1, std::min<int64_t>(kMaxGroups, (int64_t(256) << 20) / (4 * gstride)));
+  DevBuf<uint32_t> gshared((size_t)gstride * ngroups, s);
   PB_CUDA_TRY(cudaMemsetAsync(gshared.get(), 0, gshared.bytes(), s));
   DevBuf<uint8_t> state(N, s), in_near(N, s);
   LiveSide liveK, liveC;
@@ -1374,6 +1460,8 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   W.fhuge[0] = fh0.get();
   W.fhuge[1] = fh1.get();
   W.gshared = gshared.get();
+  W.gshared_stride = gstride;
+  W.ngroups = ngroups;
   W.tlist[0] = tl0.get();
   W.tlist[1] = tl1.get();
   W.gscratch = gscratch.get();
