@@ -197,8 +197,8 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
  *     modes that can hold its table (dense window, hash table, dense window + hash table); the
  *     global-scratch mode remains the fallback of endpoints none of them can hold;
  *   peeling (opts.sched = PB_SCHED_LEARNED): the setting of the persistent peel kernel — how
- *     many CTAs it runs on, how a round's CTA work is cut into units (wing), which items run on
- *     a warp and which take the whole grid (tip) — from a grid of PB_SCHED_WING_CANDIDATES (wing)
+ *     many CTAs it runs on (tip), how a round's CTA work is cut into units (wing), which items run
+ *     on a warp and which take the whole grid (tip) — from a grid of PB_SCHED_WING_CANDIDATES (wing)
  *     or PB_SCHED_TIP_CANDIDATES (tip) settings (0 = the plain setting).
  * Results are identical to the plain path's (every choice is exact).  Without an attached,
  * trained model a LEARNED call runs the plain path (stats.sched_used = 0).
@@ -209,7 +209,7 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
  * sweep the setting grid cyclically (tip and wing calls each from setting seed mod
  * the kind's number of candidates, one step per call), so that the traces cover every choice. */
 #define PB_SCHED_FEATURES 16
-#define PB_SCHED_WING_CANDIDATES 18
+#define PB_SCHED_WING_CANDIDATES 6
 #define PB_SCHED_TIP_CANDIDATES 32
 typedef enum { PB_SCHED_COUNT = 0, PB_SCHED_PEEL = 1 } pb_sched_target;
 typedef enum { PB_TRACE_OFF = 0, PB_TRACE_PLAIN = 1, PB_TRACE_EXPLORE = 2 } pb_trace_mode;

@@ -33,7 +33,7 @@ EXPORTS = [
 ]
 
 SCHED_FEATURES = 16
-SCHED_WING_CANDIDATES = 18
+SCHED_WING_CANDIDATES = 6
 SCHED_TIP_CANDIDATES = 32
 SCHED_COUNT, SCHED_PEEL = 0, 1
 TRACE_OFF, TRACE_PLAIN, TRACE_EXPLORE = 0, 1, 2

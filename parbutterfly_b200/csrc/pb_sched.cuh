@@ -7,7 +7,7 @@
 namespace pb {
 
 constexpr int kPeelCallFeatures = 12;  // call-level features; 4 candidate slots follow
-constexpr int kWingCandidates = 18;    // 3 units x 2 chunk x 3 CTA counts
+constexpr int kWingCandidates = 6;     // 3 units x 2 chunk (full grid)
 constexpr int kTipCandidates = 32;     // 2 small x 4 grid-level thresholds x 4 CTA counts
 
 int peel_candidates(bool wing);
