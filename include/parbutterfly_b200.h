@@ -264,8 +264,11 @@ pb_status pb_batch_destroy(pb_batch* batch);
  * file-scope device array of PB_NOALLOC_SCRATCH_BYTES, reserved on every GPU that loads the
  * library until the process exits.  Limit: max(nv, nu) <= PB_NOALLOC_MAX_SIDE, else PB_ETOOBIG
  * (message in msg when msg_len > 0).  The graph must satisfy pb_graph_upload's contract; it is
- * not validated.  The first call on a device resolves the array's device address with that
- * device current; make that first call before any stream capture.  Calls share the array:
+ * not validated.  *total must be 8-byte-aligned device memory (else PB_EINVAL).  The first
+ * call on a device resolves the array's device address with that device current and keeps it
+ * for the life of the process; make that first call before any stream capture, and do not call
+ * the entry point on a device after cudaDeviceReset there (the kept address is then stale).
+ * Calls share the array:
  * calls that overlap on the GPU (other streams, other host threads) race and give wrong
  * results.  Asynchronous: *total is ready when `stream` reaches this point. */
 #define PB_NOALLOC_SCRATCH_BYTES (16u << 20)

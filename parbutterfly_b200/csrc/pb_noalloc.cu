@@ -114,7 +114,9 @@ __global__ void noalloc_total_kernel(const uint32_t* __restrict__ offV, const ui
   if (lane == 0 && acc) atomicAdd(reinterpret_cast<unsigned long long*>(total), (unsigned long long)acc);
 }
 
-// Device address of the scratch array, resolved once per device with that device current.
+// Device address of the scratch array, resolved once per device with that device current and
+// kept for the life of the process (a cudaDeviceReset on that device makes it stale; the
+// header says so).
 std::mutex g_addr_mu;
 uint32_t* g_addr[64] = {nullptr};
 
@@ -147,6 +149,8 @@ using namespace pb;
 extern "C" pb_status pb_count_total_noalloc(const pb_csr* g, void* stream, int64_t* total, char* msg, size_t msg_len) {
   if (msg && msg_len) msg[0] = '\0';
   if (!g || !total) return fail(msg, msg_len, PB_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(total) & 7u)
+    return fail(msg, msg_len, PB_EINVAL, "pb_count_total_noalloc: total must be 8-byte aligned");
   if (g->nv < 0 || g->nu < 0 || g->m < 0) return fail(msg, msg_len, PB_EINVAL, "negative size");
   const int64_t nmax = g->nv > g->nu ? g->nv : g->nu;
   const size_t avail = kNoAllocWords - kHeaderWords;

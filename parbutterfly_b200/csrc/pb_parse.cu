@@ -24,7 +24,7 @@ __device__ __forceinline__ bool is_digit(unsigned char c) { return c >= '0' && c
 __device__ __forceinline__ bool is_space(unsigned char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t'; }
 
 __global__ void count_tokens_kernel(const unsigned char* __restrict__ t, int64_t len, int64_t nchunks,
-                                    uint32_t* counts, uint32_t* bad) {
+                                    int64_t* counts, uint32_t* bad) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = c * kChunk, e = min(len, b + kChunk);
     uint32_t n = 0, badc = 0;
@@ -42,7 +42,7 @@ __global__ void count_tokens_kernel(const unsigned char* __restrict__ t, int64_t
 }
 
 __global__ void parse_tokens_kernel(const unsigned char* __restrict__ t, int64_t len, int64_t nchunks,
-                                    const uint32_t* __restrict__ first, uint64_t* vals, int64_t cap, uint32_t* bad) {
+                                    const int64_t* __restrict__ first, uint64_t* vals, int64_t cap, uint32_t* bad) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = c * kChunk, e = min(len, b + kChunk);
     int64_t k = first[c];
@@ -113,16 +113,19 @@ void parse_adjacency_hypergraph(const char* text, size_t len, bool on_device, Pa
   }
   const int64_t nchunks = (blen + kChunk - 1) / kChunk;
   PB_REQUIRE(nchunks > 0, PB_EIO, "Bad input file: nothing after the header");
-  DevBuf<uint32_t> counts(nchunks + 1, s), bad(1, s);
+  // Token counts per chunk and their prefix are 64-bit: a valid file near the 32-bit edge limit
+  // has more than 2^32 tokens.
+  DevBuf<int64_t> counts(nchunks + 1, s);
+  DevBuf<uint32_t> bad(1, s);
   PB_CUDA_TRY(cudaMemsetAsync(bad.get(), 0, sizeof(uint32_t), s));
   PB_CUDA_TRY(cudaMemsetAsync(counts.get(), 0, counts.bytes(), s));
   PB_LAUNCH(count_tokens_kernel, grid_for(nchunks), 256, 0, s, t, blen, nchunks, counts.get(), bad.get());
-  exclusive_scan_u32(counts.get(), counts.get(), nchunks, s);
+  exclusive_scan_i64(counts.get(), counts.get(), nchunks, s);
+  int64_t ntok = 0;
   uint32_t hb[2];
-  readback(&hb[0], counts.get() + nchunks, sizeof(uint32_t), s);
+  readback(&ntok, counts.get() + nchunks, sizeof(int64_t), s);
   readback(&hb[1], bad.get(), sizeof(uint32_t), s);
   PB_REQUIRE(hb[1] == 0, PB_EIO, "Bad input file: a character that is neither a digit nor whitespace");
-  const int64_t ntok = hb[0];
   PB_REQUIRE(ntok >= 4, PB_EIO, "Bad input file: fewer than four sizes after the header");
   DevBuf<uint64_t> vals(ntok, s);
   PB_LAUNCH(parse_tokens_kernel, grid_for(nchunks), 256, 0, s, t, blen, nchunks, counts.get(), vals.get(), ntok,

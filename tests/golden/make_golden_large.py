@@ -1,0 +1,111 @@
+"""Regenerates tests/golden/golden_large.npz from the REFERENCE ITSELF, at the benchmark's sizes.
+
+Run in a checkout where the reference tree is present and oracle/_ref/ref_harness_omp has been
+built (`make -C oracle`).  Each graph comes from the library's seeded generators (the same
+calls the benchmark and the GPU tests make); the compiled reference (oracle/ref_harness.cpp over
+the unmodified ParButterfly headers) counts and peels it, and the results are stored either in
+full (the 2^18-edge R-MAT sample of the benchmark workload) or as SHA-256 digests of the dense
+little-endian int64 result plus a seeded sample of entries (the larger graphs).  The digest of
+each graph's four CSR arrays is stored too, so a test can tell a generator change from a
+counting error.
+
+Records (the reference's flags in brackets):
+  rmat18   : R-MAT 2^14 x 2^12, m = 2^18, (.55,.15,.15,.15), seed 2 — the benchmark workload's
+             generator and flags at 1/64 of the edges [-rankType ACOCORE -per EDGE -countType HASH,
+             wing peel -peelType BATCHS]: per-edge counts and wing numbers in full.
+  rmat16   : R-MAT 2^16 x 2^14, m = 2^20, same parameters [-rankType ADEG -per VERT -countType
+             BATCHS, tip peel BATCHS]: per-vertex counts and tip numbers (digests).
+  plaw10m  : |U| = 1e6 power-law degrees (alpha 2, capped at |V| = 1e5), m = 1e7, seed 3 — the
+             skewed Zipf-degree workload at 1/10 of its edges [ADEG, VERT, BATCHS, tip BATCHS]:
+             per-vertex counts and tip numbers (digests).  Its largest count exceeds 2^32; the
+             reference's 32-bit buckets still give the 64-bit answer on this graph (the C
+             restatement, with 64-bit buckets, agrees).
+  c2count  : the full benchmark graph, R-MAT 2^20 x 2^18, m = 2^24, seed 2 [ACOCORE, EDGE, HASH]:
+             per-edge counts (digest) and the total.  Its wing peel does not finish within hours
+             on the reference, so wing numbers at this size are not recorded.
+
+Usage: python tests/golden/make_golden_large.py [--skip-c2] [--threads N]
+"""
+import argparse
+import hashlib
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from parbutterfly_b200.graph import BipartiteGraph  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden_large.npz")
+SAMPLE = 4096
+
+
+def digest(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<i8").tobytes()).hexdigest()
+
+
+def graph_digest(g) -> str:
+    h = hashlib.sha256()
+    h.update(np.array([g.nv, g.nu, g.m], dtype="<i8").tobytes())
+    for a in (g.offsetsV, g.edgesV, g.offsetsU, g.edgesU):
+        h.update(np.ascontiguousarray(a, dtype="<u4").tobytes())
+    return h.hexdigest()
+
+
+GRAPHS = {
+    "rmat18": lambda: BipartiteGraph.rmat(14, 12, 1 << 18, 0.55, 0.15, 0.15, 0.15, 2),
+    "rmat16": lambda: BipartiteGraph.rmat(16, 14, 1 << 20, 0.55, 0.15, 0.15, 0.15, 2),
+    "plaw10m": lambda: BipartiteGraph.powerlaw_u(100_000, 1_000_000, 10_000_000, 2.0, 100_000, 3),
+    "c2count": lambda: BipartiteGraph.rmat(20, 18, 1 << 24, 0.55, 0.15, 0.15, 0.15, 2),
+}
+FLAGS = {
+    "rmat18": ("EDGE", "HASH", "ACOCORE", "BATCHS"),
+    "rmat16": ("VERT", "BATCHS", "ADEG", "BATCHS"),
+    "plaw10m": ("VERT", "BATCHS", "ADEG", "BATCHS"),
+    "c2count": ("EDGE", "HASH", "ACOCORE", "NONE"),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--skip-c2", action="store_true")
+    ap.add_argument("--threads", type=int, default=os.cpu_count())
+    a = ap.parse_args()
+    assert oracle.have_reference(), "build oracle/_ref first (make -C oracle)"
+    out = {}
+    if os.path.exists(OUT):
+        with np.load(OUT) as z:
+            out.update({k: z[k] for k in z.files})
+    for name, make in GRAPHS.items():
+        if a.skip_c2 and name == "c2count":
+            continue
+        g = make()
+        per, ct, rank, peel = FLAGS[name]
+        t0 = time.time()
+        r = oracle.run_reference(g, per, ct, rank, peel, threads=a.threads)
+        out[f"{name}/graph_sha"] = np.array(graph_digest(g))
+        out[f"{name}/flags"] = np.array(" ".join(FLAGS[name]))
+        out[f"{name}/use_v_wside_total"] = np.array([int(r["use_v"]), r["w_side"], r["total"]], dtype=np.int64)
+        out[f"{name}/count_sha"] = np.array(digest(r["count"]))
+        rng = np.random.default_rng(1234)
+        idx = np.sort(rng.choice(r["count"].size, size=min(SAMPLE, r["count"].size), replace=False))
+        out[f"{name}/sample_idx"] = idx.astype(np.int64)
+        out[f"{name}/count_sample"] = r["count"][idx]
+        if r["peel"] is not None:
+            out[f"{name}/peel_sha"] = np.array(digest(r["peel"]))
+            out[f"{name}/peel_sample"] = r["peel"][idx]
+        if name == "rmat18":  # in full: the benchmark workload's small sample
+            assert r["count"].max() < 2 ** 32 and r["peel"].max() < 2 ** 32
+            out[f"{name}/count"] = r["count"].astype(np.uint32)
+            out[f"{name}/peel"] = r["peel"].astype(np.uint32)
+        print(f"{name}: nv={g.nv} nu={g.nu} m={g.m} total={r['total']} count_s={r['count_s']:.2f} "
+              f"peel_s={r['peel_s']:.2f} wall={time.time() - t0:.1f}s", flush=True)
+        np.savez_compressed(OUT, **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -2,16 +2,18 @@
 
 It serves callers that cannot call cudaMalloc where they need a count (code inside another
 framework's memory pool, paths that must not synchronise the device, callers near the memory
-limit).  Its output is checked against the existing pb_count_total entry point, exactly
-(integer counts), on two calls in a row: the static scratch array keeps the previous call's
-contents, so the second call also checks that the entry point clears what must start at zero.
-This file is collected last on purpose.
+limit).  Its output is checked, exactly (integer counts), against the existing pb_count_total
+entry point, against the CPU oracle's total and, for the fixtures produced by the reference
+itself, against the reference's own total, on two calls in a row: the static scratch array
+keeps the previous call's contents, so the second call also checks that the entry point clears
+what must start at zero.  This file is collected last on purpose.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
+import oracle
 from parbutterfly_b200 import _ffi
 from parbutterfly_b200 import butterflies as pb
 from parbutterfly_b200.graph import BipartiteGraph
@@ -49,11 +51,21 @@ def test_noalloc_total_matches_count_total_twice(make):
         dg = ctx.upload(g)
         expect = pb.count_total(dg, "BATCHS", "ADEG")
         dg.close()
+    assert expect == oracle.count(g, "TOTAL", "ADEG")[0]
     s, keep = _device_csr(g)
     first = _noalloc_total(s)
     second = _noalloc_total(s)
     assert first == expect
     assert second == expect
+
+
+def test_noalloc_total_matches_reference_golden(golden):
+    # Totals the reference itself printed for the fixture graphs (BATCHS, ADEG).
+    for name, (g, rec) in golden.items():
+        expect = int(rec["TOTAL/BATCHS/ADEG"][0])
+        s, keep = _device_csr(g)
+        for _ in range(2):
+            assert _noalloc_total(s) == expect, name
 
 
 def test_noalloc_rejects_oversized_side():
