@@ -22,9 +22,14 @@ Records (the reference's flags in brackets):
              restatement, with 64-bit buckets, agrees).
   c2count  : the full benchmark graph, R-MAT 2^20 x 2^18, m = 2^24, seed 2 [ACOCORE, EDGE, HASH]:
              per-edge counts (digest) and the total.  Its wing peel does not finish within hours
-             on the reference, so wing numbers at this size are not recorded.
+             on the reference, so the reference's own wing numbers at this size are not recorded.
+  c2wing   : (--c2-wing) wing numbers of the full benchmark graph from the C restatement's
+             bucket-queue wing peel (oracle/pb_oracle_fast.c), run on per-edge counts whose
+             digest equals the reference's c2count digest.  The restatement is pinned to the
+             reference's own wing numbers on every golden graph and on rmat18; this record is
+             the restatement's output, not the reference's (provenance stored with it).
 
-Usage: python tests/golden/make_golden_large.py [--skip-c2] [--threads N]
+Usage: python tests/golden/make_golden_large.py [--skip-c2] [--c2-wing] [--threads N]
 """
 import argparse
 import hashlib
@@ -73,8 +78,12 @@ FLAGS = {
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-c2", action="store_true")
+    ap.add_argument("--c2-wing", action="store_true", help="only add the c2wing record (needs c2count)")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     a = ap.parse_args()
+    if a.c2_wing:
+        c2_wing(a.threads)
+        return
     assert oracle.have_reference(), "build oracle/_ref first (make -C oracle)"
     out = {}
     if os.path.exists(OUT):
@@ -105,6 +114,31 @@ def main():
         print(f"{name}: nv={g.nv} nu={g.nu} m={g.m} total={r['total']} count_s={r['count_s']:.2f} "
               f"peel_s={r['peel_s']:.2f} wall={time.time() - t0:.1f}s", flush=True)
         np.savez_compressed(OUT, **out)
+
+
+def c2_wing(threads):
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    with np.load(OUT) as z:
+        out = {k: z[k] for k in z.files}
+    g = GRAPHS["c2count"]()
+    assert graph_digest(g) == str(out["c2count/graph_sha"])
+    t0 = time.time()
+    c, _ = oracle.count(g, "EDGE", "ACOCORE")
+    assert digest(c) == str(out["c2count/count_sha"]), "oracle counts differ from the reference's"
+    t1 = time.time()
+    wing, rounds = oracle.peel_edge_fast(g, c)
+    t2 = time.time()
+    rng = np.random.default_rng(1234)
+    idx = np.sort(rng.choice(wing.size, size=SAMPLE, replace=False))
+    out["c2wing/graph_sha"] = out["c2count/graph_sha"]
+    out["c2wing/provenance"] = np.array("oracle/pb_oracle_fast.c bucket-queue wing peel of the reference-matching "
+                                        "per-edge counts (c2count digest)")
+    out["c2wing/peel_sha"] = np.array(digest(wing))
+    out["c2wing/sample_idx"] = idx.astype(np.int64)
+    out["c2wing/peel_sample"] = wing[idx]
+    out["c2wing/rounds_max"] = np.array([rounds, int(wing.max())], dtype=np.int64)
+    np.savez_compressed(OUT, **out)
+    print(f"c2wing: count {t1 - t0:.1f}s wing {t2 - t1:.1f}s rounds {rounds} max {int(wing.max())}", flush=True)
 
 
 if __name__ == "__main__":

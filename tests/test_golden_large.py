@@ -20,6 +20,8 @@ import pytest
 from parbutterfly_b200.graph import BipartiteGraph
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_large.npz")
+MODEL = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "parbutterfly_b200", "models",
+                     "sched_b200.bin")
 
 GRAPHS = {
     "rmat18": lambda: BipartiteGraph.rmat(14, 12, 1 << 18, 0.55, 0.15, 0.15, 0.15, 2),
@@ -83,11 +85,18 @@ def test_rmat18_benchmark_flags_count_and_wing(ctx, large):
         np.testing.assert_array_equal(e, r["count"].astype(np.int64))
         wing = pb.peel_e(dg, e)
         np.testing.assert_array_equal(wing, r["peel"].astype(np.int64))
-        # Learned scheduling changes how the work runs, never the result.
-        e2 = pb.count_e(dg, "HASH", "ACOCORE", sched="learned")
-        np.testing.assert_array_equal(e2, e)
-        wing2 = pb.peel_e(dg, e, sched="learned")
-        np.testing.assert_array_equal(wing2, wing)
+        # Learned scheduling (the shipped cost models) changes how the work runs, never the result.
+        model = pb.SchedModel(ctx)
+        model.load(MODEL)
+        model.attach()
+        try:
+            e2 = pb.count_e(dg, "HASH", "ACOCORE", sched="learned")
+            np.testing.assert_array_equal(e2, e)
+            wing2 = pb.peel_e(dg, e, sched="learned")
+            np.testing.assert_array_equal(wing2, wing)
+        finally:
+            pb.detach_sched_model(ctx)
+            model.close()
     finally:
         dg.close()
 

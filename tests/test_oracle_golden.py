@@ -44,6 +44,9 @@ def test_golden_wing_numbers(golden):
         c, _ = oracle.count(g, "EDGE", "ADEG")
         wing, rounds = oracle.peel_edge(g, c)
         np.testing.assert_array_equal(wing, rec["wing"], err_msg=name)
+        fast, rounds_fast = oracle.peel_edge_fast(g, c)
+        np.testing.assert_array_equal(fast, rec["wing"], err_msg=name)
+        assert rounds_fast == rounds, name
 
 
 @pytest.mark.parametrize("a,b", [(2, 2), (3, 4), (5, 7), (6, 3)])
