@@ -66,7 +66,13 @@ typedef struct {
                              signature times every candidate, later calls on the context reuse
                              the fastest (results are identical either way) */
   int32_t use_v;          /* -1 = choose as cmpWedgeCounts does; 0/1 forces the count side */
-  int32_t reserved;
+  int32_t peel_parts;     /* batching of the peel's exact rounds (no counterpart in the reference;
+                             results are identical either way): 0 = the scheduler's choice when
+                             sched = LEARNED, else one round at a time over the whole GPU;
+                             n > 0 = the two-phase schedule with about n partitions (a coarse
+                             pass cuts the items by ranges of their final numbers, then every
+                             partition runs its exact rounds independently, all in one launch);
+                             -1 = one round at a time even when sched = LEARNED */
 } pb_opts;
 
 /* Host-side two-sided CSR, the layout of struct bipartiteCSR (butterfly_utils.h:184-197).
@@ -117,6 +123,11 @@ typedef struct {
   int32_t count_blocks_per_sm; /* CTAs per SM */
   int32_t count_small_w;       /* endpoints with at most this many wedges go to a warp */
   int32_t autotuned;           /* 1 when this call ran the autotuner's sweep */
+  /* Round batching of the last peel call (two-phase schedule; zeros when it ran one round at a
+   * time): partitions, rounds of the coarse pass, rounds of the longest partition. */
+  int64_t peel_parts;
+  int64_t peel_coarse_rounds;
+  int64_t peel_fine_rounds_max;
 } pb_stats;
 
 typedef struct pb_ctx pb_ctx;

@@ -53,7 +53,7 @@ class Opts(C.Structure):
     _fields_ = [
         ("count_type", C.c_int32), ("rank_type", C.c_int32), ("peel_type", C.c_int32),
         ("per_type", C.c_int32), ("max_wedges", C.c_int64), ("max_array_size", C.c_int64),
-        ("sched", C.c_int32), ("autotune", C.c_int32), ("use_v", C.c_int32), ("reserved", C.c_int32),
+        ("sched", C.c_int32), ("autotune", C.c_int32), ("use_v", C.c_int32), ("peel_parts", C.c_int32),
     ]
 
 
@@ -75,6 +75,7 @@ class Stats(C.Structure):
         ("ms_sched", C.c_double), ("sched_pred", C.c_double), ("sched_meas", C.c_double),
         ("sched_mae_log2", C.c_double), ("count_smem_bytes", C.c_int32), ("count_blocks_per_sm", C.c_int32),
         ("count_small_w", C.c_int32), ("autotuned", C.c_int32),
+        ("peel_parts", C.c_int64), ("peel_coarse_rounds", C.c_int64), ("peel_fine_rounds_max", C.c_int64),
     ]
 
 

@@ -41,7 +41,11 @@ def _enum(table, v, what):
 
 
 def make_opts(count_type="SERIAL", rank_type="ADEG", peel_type="BATCHS", per="VERT", use_v: Optional[bool] = None,
-              max_wedges=2577500000, max_array_size=23090996160, sched="plain", autotune=False) -> _ffi.Opts:
+              max_wedges=2577500000, max_array_size=23090996160, sched="plain", autotune=False,
+              peel_parts=0) -> _ffi.Opts:
+    """pb_opts.  peel_parts: batching of the peel's exact rounds (0: the scheduler's choice when
+    sched="learned", else one round at a time; n > 0: the two-phase schedule with about n
+    partitions; -1: one round at a time even when learned).  Results never depend on it."""
     o = _ffi.Opts()
     _ffi.lib().pb_opts_default(C.byref(o))
     o.count_type = _enum(COUNT_TYPES, count_type, "count type")
@@ -53,6 +57,7 @@ def make_opts(count_type="SERIAL", rank_type="ADEG", peel_type="BATCHS", per="VE
     o.sched = 1 if str(sched).lower() == "learned" else 0
     o.autotune = 1 if autotune else 0
     o.use_v = -1 if use_v is None else int(bool(use_v))
+    o.peel_parts = int(peel_parts)
     return o
 
 

@@ -158,6 +158,7 @@ pb_opts resolve_opts(const pb_opts* o) {
   PB_REQUIRE(r.peel_type >= PB_PSORT && r.peel_type <= PB_PBATCHWA, PB_EINVAL, "peel_type out of range");
   PB_REQUIRE(r.per_type >= PB_VERT && r.per_type <= PB_TOTAL, PB_EINVAL, "per_type out of range");
   PB_REQUIRE(r.sched == PB_SCHED_PLAIN || r.sched == PB_SCHED_LEARNED, PB_EINVAL, "sched out of range");
+  PB_REQUIRE(r.peel_parts >= -1, PB_EINVAL, "peel_parts out of range");
   return r;
 }
 
@@ -422,7 +423,13 @@ PeelTuning peel_setting(pb_ctx* ctx, const pb_graph& g, int use_v, bool wing, co
   st.sched_choice = 0;
   st.ms_sched = 0;
   st.sched_pred = 0;
-  const bool learned = o.sched == PB_SCHED_LEARNED && ctx->model && ctx->model->peel.trained;
+  if (o.peel_parts > 0) {  // the caller fixes the round batching
+    PeelTuning t = plain_peel_tuning(wing);
+    t.two_phase = true;
+    t.parts_total = o.peel_parts;
+    return t;
+  }
+  const bool learned = o.peel_parts == 0 && o.sched == PB_SCHED_LEARNED && ctx->model && ctx->model->peel.trained;
   if (!learned && ctx->trace_mode == PB_TRACE_OFF) return plain_peel_tuning(wing);
   auto t0 = std::chrono::steady_clock::now();
   float f[kPeelCallFeatures];
@@ -763,6 +770,9 @@ static pb_status peel_entry(pb_ctx* ctx, const pb_graph* g, const pb_opts* opts,
       ctx->stats.ms_peel = T.ms(0, 1);
       ctx->stats.peel_rounds = pr.rounds;
       ctx->stats.peel_work = pr.work;
+      ctx->stats.peel_parts = pr.parts;
+      ctx->stats.peel_coarse_rounds = pr.coarse_rounds;
+      ctx->stats.peel_fine_rounds_max = pr.fine_rounds_max;
       ctx->stats.sched_meas = ctx->stats.ms_peel;
       log_peel_trace(ctx, row, ctx->stats.ms_peel);
     });

@@ -107,8 +107,11 @@ void build_union(const pb_graph* const* gs, int k, pb_graph& U, std::vector<int6
 
 // Peeling stage (pb_peel.cu).
 struct PeelResult {
-  int64_t rounds = 0;
+  int64_t rounds = 0;           // exact bucket rounds (summed over the partitions of a two-phase peel)
   int64_t work = 0;
+  int64_t coarse_rounds = 0;    // two-phase: rounds of the coarse pass
+  int64_t parts = 0;            // two-phase: partitions
+  int64_t fine_rounds_max = 0;  // two-phase: rounds of the longest partition
 };
 // Work-unit sizing of the persistent peel kernel (the defaults are the plain path's).
 struct PeelTuning {
@@ -119,6 +122,13 @@ struct PeelTuning {
   int64_t near_min = 32768;               // the near window holds at least this many items
   int64_t near_div = 64;                  // ... or alive / near_div
   int64_t max_ctas = 0;                   // CTAs of the persistent kernel (0: all resident)
+  // Two-phase schedule: a coarse pass cuts the items into partitions (ranges of their final
+  // numbers, about parts_per_cta per CTA or parts_total in all, of equal estimated work), then
+  // every partition runs its exact rounds as an independent instance of one launch.  Same
+  // results as one instance running every round over the whole GPU.
+  bool two_phase = false;
+  double parts_per_cta = 2.0;
+  int64_t parts_total = 0;
 };
 // The plain path's settings: wing items never take the whole grid; tip items above 2^13
 // wedges do (one CTA per heavy vertex leaves the rest of the GPU idle in most rounds).

@@ -19,6 +19,8 @@
 // pass over the alive list, a log2 histogram of distances to the minimum) when the near list
 // runs dry.  Frontier items with little work run one per warp; heavy ones one per CTA.
 #include <algorithm>
+#include <functional>
+#include <memory>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -70,6 +72,14 @@ struct Ctl {
   unsigned near_min, near_div;
   // Barriers of CTA groups that process heavy tip items concurrently.
   unsigned gbar_count[32], gbar_gen[32];
+  // Range mode (the coarse pass of the two-phase peel): each window is one partition, its
+  // frontier every unpeeled item whose count is below the window bound, repeated until no
+  // unpeeled item is below it.  The bound is chosen so that the window holds about
+  // part_target of estimated work.  npart counts the partitions opened so far.
+  unsigned range_mode, npart;
+  unsigned long long part_target;
+  unsigned long long whist[66];    // estimated work per log2 distance bin
+  unsigned long long wsub[256];    // estimated work per linear sub-bin of the chosen octave
 };
 constexpr unsigned kMaxGroups = 32;
 
@@ -112,7 +122,18 @@ struct Work {
   uint32_t* gscratch;  // per-CTA dense scratch (dense counters / probe markers)
   int64_t gscratch_len;
   int64_t N;           // items of this instance
-  uint32_t item0;      // first item id of this instance (its items are item0 .. item0 + N - 1)
+  uint32_t item0;      // first item of this instance: its items are items[item0 .. item0 + N)
+                       // (item0 .. item0 + N - 1 themselves when items is null)
+  const uint32_t* items;
+  // Two-phase peel.  Fine pass: every instance is one partition of the coarse pass; part[x]
+  // is the partition of item x and my_part this instance's.  Items of lower partitions are
+  // peeled, items of higher partitions stay unpeeled for the whole pass (and are never
+  // charged), items of my_part follow the exact rounds.  Coarse pass: part_out receives the
+  // partition of every item as it is peeled.  level: the live-list version the instance reads.
+  const uint32_t* part;
+  uint32_t my_part;
+  uint32_t* part_out;
+  uint32_t level;
 };
 
 // Every CTA belongs to one peel instance (the whole input, or one graph of a batch, each with
@@ -150,6 +171,10 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int ph, unsigned long long 
 // Bounded: a wait longer than the control block's timeout sets ERR_TIMEOUT and returns false.
 __device__ bool grid_barrier(Ctl* ctl) {
   __shared__ int ok;
+  if (vgrid() == 1) {  // one CTA: a block barrier orders its global memory accesses too
+    __syncthreads();
+    return *(volatile unsigned*)&ctl->err == 0;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = &ctl->bar_gen;
@@ -410,8 +435,10 @@ __shared__ unsigned long long s_win_hi;
 // the window bound can reach the frontier before the next window advance, so only those are
 // queued for re-bucketing; items that stay above it keep bucket == count implicitly (the
 // advance resynchronises buckets from counts, when no unpeeled item is in the near list).
+__device__ __forceinline__ bool mine(const Work& W, uint32_t x) { return !W.part || W.part[x] == W.my_part; }
+
 __device__ __forceinline__ void dec(const Work& W, Ctl* ctl, unsigned par, uint32_t x, int64_t amount) {
-  if (W.state[x] == ALIVE) {
+  if (mine(W, x) && W.state[x] == ALIVE) {
     const long long old = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&W.cnt[x]),
                                                (unsigned long long)(-amount));
     if ((unsigned long long)(old - amount) < s_win_hi) touch(W, ctl, par, x);
@@ -514,9 +541,27 @@ struct WingEdge {
   bool from_v;
 };
 
+// An edge of a lower partition is gone; one of a higher partition is present and unpeeled.
 __device__ __forceinline__ bool skip_edge(const Work& W, uint32_t e, uint32_t e1) {
+  if (W.part) {
+    const uint32_t p = W.part[e];
+    if (p != W.my_part) return p < W.my_part;
+  }
   const uint8_t s = W.state[e];
   return s == PEELED || (s == ACTIVE && e < e1);
+}
+
+__device__ __forceinline__ bool edge_gone(const Work& W, uint32_t e) {
+  if (W.part) {
+    const uint32_t p = W.part[e];
+    if (p != W.my_part) return p < W.my_part;
+  }
+  return W.state[e] == PEELED;
+}
+
+// In this round's frontier with a smaller index than e1 (the tie rule).
+__device__ __forceinline__ bool active_before(const Work& W, uint32_t e, uint32_t e1) {
+  return e < e1 && mine(W, e) && W.state[e] == ACTIVE;
 }
 
 // Item granularity: one warp, one CTA, or the whole grid (huge items; all CTAs call it).
@@ -549,7 +594,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     uint32_t key, e;
     if (E.from_v) { key = G.edgK[p]; e = G.eidK[p]; }
     else { key = G.edgC[p]; e = G.eidC[p]; }
-    if (W.state[e] == PEELED) continue;
+    if (edge_gone(W, e)) continue;
     if (hash) t_put(keys, vals, mask, key, e, ctl);
     else mark[key] = e + 1;
   }
@@ -618,7 +663,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       uint32_t e4;
       if (!probe(v2, e4)) return;  // most probes miss: test the table before any global read
       const uint32_t e3 = G.eidK[q];
-      if (skip_edge(W, e3, E.e1) || (W.state[e4] == ACTIVE && e4 < E.e1)) return;
+      if (skip_edge(W, e3, E.e1) || active_before(W, e4, E.e1)) return;
       found(p, e3, e4);
     };
     const uint32_t b1 = G.offC[E.v], d1 = G.offC[E.v + 1] - b1;
@@ -653,7 +698,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       uint32_t e2;
       if (!probe(u2, e2)) return;
       const uint32_t e3 = G.eidC[p3];
-      if (skip_edge(W, e3, E.e1) || (W.state[e2] == ACTIVE && e2 < E.e1)) return;
+      if (skip_edge(W, e3, E.e1) || active_before(W, e2, E.e1)) return;
       found(q, e2, e3);
     };
     const uint32_t b1 = G.offK[E.u], d1 = G.offK[E.u + 1] - b1;
@@ -773,6 +818,18 @@ struct Classify {
   }
 };
 
+// Estimated work of peeling item x (plus one, so that items without work still count): the
+// cheaper side's two-hop probes of a wing item, the two-hop wedges of a tip item.
+template <bool kWing>
+__device__ __forceinline__ unsigned long long item_weight(const Lists& G, const Classify& cls, uint32_t x) {
+  if (kWing) {
+    const uint32_t v = G.center_of[x], u = G.u_of[x];
+    const int64_t c = min(cls.cost_v(G, v, u), cls.cost_u(G, v, u));
+    return 1ull + (unsigned long long)(c > 0 ? c : 0);
+  }
+  return 1ull + (unsigned long long)(G.wk[x] > 0 ? G.wk[x] : 0);
+}
+
 // The peel instances of one launch.  n == 1: the whole grid runs instance 0.  Otherwise CTA b
 // runs instances cta_beg[b] .. cta_end[b] - 1 one after another; instance i spans the ncta[i]
 // CTAs from first[i] (heavy graphs get many CTAs, light graphs share one CTA in turn).
@@ -798,9 +855,12 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
   const unsigned gtid = vblock() * kPT + threadIdx.x;
   const unsigned gthreads = vgrid() * kPT;
   unsigned alist_cur = *(volatile unsigned*)&ctl->alist_cur;
+  const bool range = *(volatile unsigned*)&ctl->range_mode != 0;
+  unsigned part_idx = *(volatile unsigned*)&ctl->npart;  // partitions opened (range mode)
   unsigned long long work = 0;
   if (!*(volatile unsigned*)&ctl->started) {
-    for (int64_t x = gtid; x < W.N; x += gthreads) W.alist[0][x] = W.item0 + (uint32_t)x;
+    for (int64_t x = gtid; x < W.N; x += gthreads)
+      W.alist[0][x] = W.items ? W.items[W.item0 + x] : W.item0 + (uint32_t)x;
     if (!grid_barrier(ctl)) return false;
     if (vblock() == 0 && threadIdx.x == 0) ctl->started = 1;
   }
@@ -842,32 +902,90 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
       if (lane == 0 && mn != kInf) atomicMin(&ctl->k_lo, mn);
       if (threadIdx.x < 66) S.hist[threadIdx.x] = 0;
       if (vblock() == 0) {
-        // The previous advance's histogram was last read before two barriers ago.
-        if (threadIdx.x < 66) ctl->hist[threadIdx.x] = 0;
+        // The previous advance's histograms were last read before two barriers ago.
+        if (threadIdx.x < 66) {
+          ctl->hist[threadIdx.x] = 0;
+          ctl->whist[threadIdx.x] = 0;
+        }
+        if (range && threadIdx.x < 256) ctl->wsub[threadIdx.x] = 0;
         if (threadIdx.x == 0) ctl->near_len = 0;
       }
       if (!grid_barrier(ctl)) return false;
+      if (range) {
+        ++part_idx;  // the window opened here is partition part_idx - 1
+        if (vblock() == 0 && threadIdx.x == 0) ctl->npart = part_idx;
+      }
       const unsigned long long klo = *(volatile unsigned long long*)&ctl->k_lo;
       const unsigned alen2 = *(volatile unsigned*)&ctl->alen[na];
-      for (unsigned q = gtid; q < alen2; q += gthreads) {
-        const unsigned long long d = (unsigned long long)W.D[W.alist[na][q]] - klo;
-        atomicAdd(&S.hist[d ? 64 - __clzll(d) : 0], 1u);
-      }
-      __syncthreads();
-      if (threadIdx.x < 66 && S.hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], S.hist[threadIdx.x]);
-      if (!grid_barrier(ctl)) return false;
-      // Every CTA derives the same bound: the smallest B with >= target items at distance < 2^B.
-      const unsigned target = max(ctl->near_min, alen2 / max(1u, ctl->near_div));
-      unsigned cum = 0;
-      int B = 0;
-      for (; B < 65; ++B) {
-        cum += *(volatile unsigned*)&ctl->hist[B];
-        if (cum >= target) break;
-      }
       unsigned long long hi = kInf;
-      if (B < 63) {
-        const unsigned long long span = 1ull << B;
-        if (klo <= kInf - span) hi = klo + span;
+      if (!range) {
+        for (unsigned q = gtid; q < alen2; q += gthreads) {
+          const unsigned long long d = (unsigned long long)W.D[W.alist[na][q]] - klo;
+          atomicAdd(&S.hist[d ? 64 - __clzll(d) : 0], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x < 66 && S.hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], S.hist[threadIdx.x]);
+        if (!grid_barrier(ctl)) return false;
+        // Every CTA derives the same bound: the smallest B with >= target items at distance < 2^B.
+        const unsigned target = max(ctl->near_min, alen2 / max(1u, ctl->near_div));
+        unsigned cum = 0;
+        int B = 0;
+        for (; B < 65; ++B) {
+          cum += *(volatile unsigned*)&ctl->hist[B];
+          if (cum >= target) break;
+        }
+        if (B < 63) {
+          const unsigned long long span = 1ull << B;
+          if (klo <= kInf - span) hi = klo + span;
+        }
+      } else {
+        // Partition bound: about part_target of estimated work below it.  A log2 histogram of
+        // distances to the minimum (weighted by work) picks the octave, a 256-bin linear
+        // histogram inside it the bound.  The bins live in the (idle) table pool.
+        unsigned long long* wh = reinterpret_cast<unsigned long long*>(pool);
+        if (threadIdx.x < 66) wh[threadIdx.x] = 0;
+        __syncthreads();
+        for (unsigned q = gtid; q < alen2; q += gthreads) {
+          const uint32_t x = W.alist[na][q];
+          const unsigned long long d = (unsigned long long)W.D[x] - klo;
+          atomicAdd(&wh[d ? 64 - __clzll(d) : 0], item_weight<kWing>(G, cls, x));
+        }
+        __syncthreads();
+        if (threadIdx.x < 66 && wh[threadIdx.x]) atomicAdd(&ctl->whist[threadIdx.x], wh[threadIdx.x]);
+        if (!grid_barrier(ctl)) return false;
+        const unsigned long long target = *(volatile unsigned long long*)&ctl->part_target;
+        unsigned long long cum = 0;
+        int B = 0;
+        for (; B < 65; ++B) {
+          const unsigned long long w = *(volatile unsigned long long*)&ctl->whist[B];
+          if (cum + w >= target) break;
+          cum += w;
+        }
+        if (B == 0) {
+          hi = klo + 1;
+        } else if (B < 63) {
+          const unsigned long long lo_d = 1ull << (B - 1), width = lo_d;  // distances [2^(B-1), 2^B)
+          __syncthreads();
+          if (threadIdx.x < 256) wh[threadIdx.x] = 0;
+          __syncthreads();
+          for (unsigned q = gtid; q < alen2; q += gthreads) {
+            const uint32_t x = W.alist[na][q];
+            const unsigned long long d = (unsigned long long)W.D[x] - klo;
+            if (d >= lo_d && d < lo_d + width)
+              atomicAdd(&wh[(unsigned)((d - lo_d) * 256ull / width)], item_weight<kWing>(G, cls, x));
+          }
+          __syncthreads();
+          if (threadIdx.x < 256 && wh[threadIdx.x]) atomicAdd(&ctl->wsub[threadIdx.x], wh[threadIdx.x]);
+          if (!grid_barrier(ctl)) return false;
+          unsigned j = 0;
+          for (; j < 255; ++j) {
+            cum += *(volatile unsigned long long*)&ctl->wsub[j];
+            if (cum >= target) break;
+          }
+          // Bin j covers distances [lo_d + ceil(j w / 256), lo_d + ceil((j + 1) w / 256)).
+          const unsigned long long end_d = lo_d + ((unsigned long long)(j + 1) * width + 255ull) / 256ull;
+          if (klo <= kInf - end_d) hi = klo + end_d;
+        }
       }
       for (unsigned q = gtid; q < alen2; q += gthreads) {
         const uint32_t x = W.alist[na][q];
@@ -899,7 +1017,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         const uint32_t x = W.near[q];
         if (W.state[x] != ALIVE) continue;
         const unsigned long long d = (unsigned long long)W.D[x];
-        if (d == k) {
+        if (range || d == k) {
           W.state[x] = ACTIVE;
           bool small, huge;
           int64_t cost;
@@ -910,11 +1028,11 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             cost = fv ? cv : cu;
             const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
             small = cost <= cls.small_work && 2 * psize <= (uint32_t)kWarpSlots;
-            huge = !small && cost > cls.huge_work;
+            huge = !small && cost > cls.huge_work && W.gshared != nullptr;
           } else {
             cost = G.wk[x];
             small = cls.tip_small(G, x);
-            huge = !small && cls.tip_huge(G, x);
+            huge = !small && cls.tip_huge(G, x) && W.gshared != nullptr;
           }
           atomicAdd(&ctl->round_est[par], (unsigned long long)(cost > 0 ? cost : 0));
           if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
@@ -1113,8 +1231,9 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         W.touched[x] = 0;
         if (W.state[x] != ALIVE) continue;
         const int64_t c = W.cnt[x];
-        const int64_t nd = c > (int64_t)k ? c : (int64_t)k;
-        W.D[x] = nd;
+        // Range mode keeps D (the count at the partition's start) and queues by count.
+        const int64_t nd = range ? c : (c > (int64_t)k ? c : (int64_t)k);
+        if (!range) W.D[x] = nd;
         if ((unsigned long long)nd < win_hi) {
           mn = min(mn, (unsigned long long)nd);
           if (!W.in_near[x]) {
@@ -1132,6 +1251,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
       for (unsigned q = gtid; q < ns + nb + nh; q += gthreads) {
         const uint32_t x = q < ns ? W.fsmall[par][q] : (q < ns + nb ? W.fbig[par][q - ns] : W.fhuge[par][q - ns - nb]);
         W.state[x] = PEELED;
+        if (range) W.part_out[x] = part_idx - 1;
       }
       if (vblock() == 0 && threadIdx.x == 0) {
         ctl->alive -= ns + nb + nh;
@@ -1153,17 +1273,22 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
 }
 
 template <bool kWing>
-__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, Instances I, Ctl* ctls, Classify cls) {
+__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, const Lists* levels, Instances I, Ctl* ctls,
+                                                   Classify cls) {
+  // levels: the live-list versions of a two-phase fine pass (an instance reads
+  // levels[W.level]); null: every instance reads G.
   __shared__ Work sW;
+  __shared__ Lists sG;
   const unsigned ib = I.n > 1 ? I.cta_beg[blockIdx.x] : 0u, ie = I.n > 1 ? I.cta_end[blockIdx.x] : 1u;
   for (unsigned inst = ib; inst < ie; ++inst) {
     if (threadIdx.x == 0) {
       s_vb = I.n > 1 ? blockIdx.x - I.first[inst] : blockIdx.x;
       s_vg = I.n > 1 ? I.ncta[inst] : gridDim.x;
       sW = I.W[inst];
+      sG = levels ? levels[sW.level] : G;
     }
     __syncthreads();
-    if (!peel_instance<kWing>(G, sW, ctls + inst, cls)) return;
+    if (!peel_instance<kWing>(sG, sW, ctls + inst, cls)) return;
     __syncthreads();
   }
 }
@@ -1288,30 +1413,38 @@ __global__ void iota_kernel(uint32_t* a, int64_t n) {
 
 int grid_for(int64_t n, int per_block = 256) { return std::max(1, std::min(ceil_div(n, per_block), sm_count() * 16)); }
 
-// One side's live lists (double-buffered so a compaction can read the previous version).
+// One version of one side's live lists.
+struct ListVersion {
+  DevBuf<uint32_t> off, nbr, eid;
+};
+
+// One side's live lists: every compaction makes a new version from the current one.  With
+// keep_all (two-phase peel) every version stays: the fine pass reads, for each partition, the
+// newest version that still holds all of its items.  Otherwise only the newest stays.
 struct LiveSide {
-  DevBuf<uint32_t> off[2], nbr[2], eid[2];
-  int cur = 0;
+  std::vector<std::unique_ptr<ListVersion>> ver;
   int64_t n = 0;
+  bool keep_all = false;
 };
 
 template <bool kByEdge>
 void compact_side(LiveSide& L, const uint32_t* off, const uint32_t* nbr, const uint32_t* eid, const uint8_t* state,
                   bool with_eid, cudaStream_t s) {
-  const int nx = L.cur ^ 1;
+  auto nv = std::make_unique<ListVersion>();
   DevBuf<uint32_t> deg(L.n > 0 ? L.n : 1, s);
   if (L.n) PB_LAUNCH(live_degree_kernel<kByEdge>, grid_for(L.n * 32), 256, 0, s, off, nbr, eid, L.n, state, deg.get());
-  if (L.off[nx].n < (size_t)L.n + 1) L.off[nx].alloc(L.n + 1, s);
-  exclusive_scan_u32(deg.get(), L.off[nx].get(), L.n, s);
+  nv->off.alloc(L.n + 1, s);
+  exclusive_scan_u32(deg.get(), nv->off.get(), L.n, s);
   uint32_t live = 0;
-  PB_CUDA_TRY(cudaMemcpyAsync(&live, L.off[nx].get() + L.n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaMemcpyAsync(&live, nv->off.get() + L.n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   PB_CUDA_TRY(cudaStreamSynchronize(s));
-  if (L.nbr[nx].n < (size_t)live + 1) L.nbr[nx].alloc(live + 1, s);
-  if (with_eid && L.eid[nx].n < (size_t)live + 1) L.eid[nx].alloc(live + 1, s);
+  nv->nbr.alloc(live + 1, s);
+  if (with_eid) nv->eid.alloc(live + 1, s);
   if (L.n)
     PB_LAUNCH(compact_lists_kernel<kByEdge>, grid_for(L.n * 32), 256, 0, s, off, nbr, with_eid ? eid : nullptr, L.n,
-              state, L.off[nx].get(), L.nbr[nx].get(), with_eid ? L.eid[nx].get() : nullptr);
-  L.cur = nx;
+              state, nv->off.get(), nv->nbr.get(), with_eid ? nv->eid.get() : nullptr);
+  if (!L.keep_all) L.ver.clear();  // stream-ordered frees, after the compaction has read them
+  L.ver.push_back(std::move(nv));
 }
 
 // {error bits OR-ed, unpeeled items summed} over the control blocks of one launch.
@@ -1326,6 +1459,99 @@ __global__ void ctl_status_kernel(const Ctl* __restrict__ ctls, unsigned n, unsi
   if (threadIdx.x == 0) {
     out[0] = err;
     out[1] = alive;
+  }
+}
+
+// Per partition of the coarse pass: items and summed estimated work (the fine pass's CTA
+// shares); with part null, the totals over all items (partition 0).
+template <bool kWing>
+__global__ void part_stats_kernel(Lists G, Classify cls, const uint32_t* __restrict__ part, int64_t N,
+                                  unsigned* cnt, unsigned long long* work) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < N; x += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = part ? part[x] : 0u;
+    atomicAdd(&cnt[p], 1u);
+    atomicAdd(&work[p], item_weight<kWing>(G, cls, (uint32_t)x));
+  }
+}
+
+// Splits `grid` CTAs among instances by weight: an instance whose share is at least one CTA
+// gets a CTA range of its own (its barriers span only that range); the light ones are packed,
+// longest first onto the least-loaded CTA, into the CTAs left over, where they run one after
+// another.  Fills the launch order (slot -> instance), each slot's first CTA and CTA count,
+// and each CTA's slot range.
+void assign_ctas(const std::vector<double>& pweight, int grid, std::vector<int>& inst_of, std::vector<uint32_t>& first,
+                 std::vector<uint32_t>& cnt, std::vector<uint32_t>& cbeg, std::vector<uint32_t>& cend) {
+  const int ninst = (int)pweight.size();
+  std::vector<int> ord(ninst);
+  for (int i = 0; i < ninst; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return pweight[a] > pweight[b]; });
+  double wsum = 0;
+  for (double w : pweight) wsum += w;
+  int nheavy = 0;
+  while (nheavy < ninst && pweight[ord[nheavy]] / wsum * grid >= 1.0) ++nheavy;
+  double lw = 0;
+  for (int j = nheavy; j < ninst; ++j) lw += pweight[ord[j]];
+  int light_ctas = 0;
+  if (nheavy < ninst) light_ctas = std::min(ninst - nheavy, std::max(1, (int)std::ceil(lw / wsum * grid)));
+  // Heavy instances share the rest; demote the lightest ones while they outnumber it.
+  while (nheavy > grid - light_ctas) {
+    --nheavy;
+    if (!light_ctas) light_ctas = 1;
+  }
+  if (!nheavy) light_ctas = std::min(grid, ninst);
+  const int hbudget = grid - light_ctas;
+  std::vector<int> ncta(ninst, 0);
+  if (nheavy) {
+    double hw = 0;
+    for (int j = 0; j < nheavy; ++j) hw += pweight[ord[j]];
+    int total = 0;
+    for (int j = 0; j < nheavy; ++j) {
+      ncta[ord[j]] = std::max(1, (int)(pweight[ord[j]] / hw * hbudget));
+      total += ncta[ord[j]];
+    }
+    for (int j = 0; total < hbudget; j = (j + 1) % nheavy, ++total) ++ncta[ord[j]];
+    while (total > hbudget) {  // some instance has more than one CTA here (hbudget >= nheavy)
+      int k = ord[0];
+      for (int j = 1; j < nheavy; ++j)
+        if (ncta[ord[j]] > ncta[k]) k = ord[j];
+      --ncta[k];
+      --total;
+    }
+  }
+  inst_of.clear();
+  first.clear();
+  cnt.clear();
+  cbeg.assign(grid, 0);
+  cend.assign(grid, 0);
+  uint32_t cta = 0;
+  for (int j = 0; j < nheavy; ++j) {
+    const int i = ord[j];
+    for (int c = 0; c < ncta[i]; ++c) {
+      cbeg[cta + c] = (uint32_t)inst_of.size();
+      cend[cta + c] = (uint32_t)inst_of.size() + 1;
+    }
+    inst_of.push_back(i);
+    first.push_back(cta);
+    cnt.push_back((uint32_t)ncta[i]);
+    cta += (uint32_t)ncta[i];
+  }
+  if (nheavy < ninst) {
+    std::vector<std::vector<int>> bins(light_ctas);
+    std::vector<double> load(light_ctas, 0.0);
+    for (int j = nheavy; j < ninst; ++j) {
+      const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[b].push_back(ord[j]);
+      load[b] += pweight[ord[j]];
+    }
+    for (int b = 0; b < light_ctas; ++b, ++cta) {
+      cbeg[cta] = (uint32_t)inst_of.size();
+      for (int i : bins[b]) {
+        inst_of.push_back(i);
+        first.push_back(cta);
+        cnt.push_back(1u);
+      }
+      cend[cta] = (uint32_t)inst_of.size();
+    }
   }
 }
 
@@ -1347,15 +1573,27 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   G.edgK = edgK0;
   G.offC = offC0;
   G.edgC = edgC0;
+  const bool batch = parts && parts->base.size() > 1;
+  // Two-phase peel (a schedule of the same rounds, never a different result): a coarse pass
+  // cuts the items into partitions of about equal estimated work by ranges of their final
+  // numbers, then every partition runs its exact rounds as an independent instance.
+  bool two_phase_req = tune.two_phase;
+  double parts_per_cta = tune.parts_per_cta;
+  int64_t parts_total = tune.parts_total;
+  if (const char* e = getenv("PB_PEEL_TWO_PHASE")) {  // diagnostic hook: partitions per CTA, 0 = off
+    parts_per_cta = atof(e);
+    parts_total = 0;
+    two_phase_req = parts_per_cta > 0;
+  }
+  const bool two_phase = !batch && two_phase_req && g_recorder == nullptr;
 
-  DevBuf<int64_t> cnt(N, s), wk, Sx;
+  DevBuf<int64_t> cnt(N, s);
   DevBuf<uint32_t> eti, iota, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
   DevBuf<uint32_t> fs0(N, s), fs1(N, s), fb0(N, s), fb1(N, s), fh0(N, s), fh1(N, s), tl0(N, s), tl1(N, s);
   // Independent instances (the graphs of a batch) or the whole input as one.
   std::vector<int64_t> pbase{0}, psize{N};
   std::vector<double> pweight{1.0};
-  if (parts && parts->base.size() > 1) {
-    PB_REQUIRE(!kWing, PB_EUNSUPPORTED, "per-graph peel instances are built for tip peeling");
+  if (batch) {
     pbase.clear();
     psize.clear();
     pweight.clear();
@@ -1367,9 +1605,6 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     }
     if (pbase.empty()) return res;
   }
-  const int ninst = (int)pbase.size();
-  const bool multi = ninst > 1;
-  DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + ninst, s);
   // Grid-shared dense counters: tip peeling keeps one slice per CTA group (heavy items of a round
   // run concurrently), up to 32 slices within 256 MB.
   const int64_t gstride = std::max(G.nK, G.nC) + 1;
@@ -1381,16 +1616,31 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   LiveSide liveK, liveC;
   liveK.n = G.nK;
   liveC.n = G.nC;
-  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, out, cnt.get(), state.get(), in_near.get(),
-            touched.get());
-  auto refresh_work = [&]() {
+  liveK.keep_all = liveC.keep_all = two_phase;
+  DevBuf<int64_t> snap;  // two-phase: every item's count when its partition opens
+  DevBuf<uint32_t> part;
+  if (two_phase) {
+    snap.alloc(N, s);
+    part.alloc(N, s);
+  }
+  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, two_phase ? snap.get() : out, cnt.get(), state.get(),
+            in_near.get(), touched.get());
+  // Work estimates of the lists a version holds: neighbour-degree sums (wing) or two-hop wedges
+  // (tip).
+  std::vector<std::unique_ptr<DevBuf<int64_t>>> work_bufs;
+  auto refresh_work = [&](Lists& L) {
+    auto buf = std::make_unique<DevBuf<int64_t>>(kWing ? L.nK + L.nC : L.nK, s);
     if (kWing) {
-      if (G.nK) PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, Sx.get());
-      if (G.nC)
-        PB_LAUNCH(nbr_degree_sum_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.edgC, G.offK, G.nC, Sx.get() + G.nK);
+      if (L.nK) PB_LAUNCH(nbr_degree_sum_kernel, grid_for(L.nK * 32), 256, 0, s, L.offK, L.edgK, L.offC, L.nK, buf->get());
+      if (L.nC)
+        PB_LAUNCH(nbr_degree_sum_kernel, grid_for(L.nC * 32), 256, 0, s, L.offC, L.edgC, L.offK, L.nC, buf->get() + L.nK);
+      L.S = buf->get();
     } else {
-      PB_LAUNCH(tip_work_kernel, grid_for(G.nK * 32), 256, 0, s, G.offK, G.edgK, G.offC, G.nK, wk.get());
+      PB_LAUNCH(tip_work_kernel, grid_for(L.nK * 32), 256, 0, s, L.offK, L.edgK, L.offC, L.nK, buf->get());
+      L.wk = buf->get();
     }
+    if (!two_phase) work_bufs.clear();
+    work_bufs.push_back(std::move(buf));
   };
   bool need_scratch = false;
   int64_t scratch_len = 0;
@@ -1398,7 +1648,6 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     eti.alloc(g.m, s);
     iota.alloc(g.m, s);
     center_of.alloc(g.m, s);
-    Sx.alloc(G.nK + G.nC, s);
     edge_to_idxs(g, use_v, eti.get(), s);
     PB_LAUNCH(iota_kernel, grid_for(g.m), 256, 0, s, iota.get(), g.m);
     PB_LAUNCH(center_of_kernel, grid_for(G.nC * 32), 256, 0, s, G.offC, G.nC, center_of.get());
@@ -1406,22 +1655,20 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     G.eidC = iota.get();
     G.center_of = center_of.get();
     G.u_of = edgC0;  // edge ids are positions in the centre side's original lists
-    G.S = Sx.get();
-    refresh_work();
+    refresh_work(G);
     need_scratch = 2ull * g.max_deg > (uint64_t)kBlockSlots;
     scratch_len = std::max(G.nK, G.nC);
   } else {
-    wk.alloc(G.nK, s);
-    G.wk = wk.get();
-    refresh_work();
+    refresh_work(G);
     DevBuf<unsigned long long> mx(1, s);
     PB_CUDA_TRY(cudaMemsetAsync(mx.get(), 0, sizeof(unsigned long long), s));
-    PB_LAUNCH(max_i64_kernel, grid_for(G.nK), 256, 0, s, wk.get(), G.nK, mx.get());
+    PB_LAUNCH(max_i64_kernel, grid_for(G.nK), 256, 0, s, G.wk, G.nK, mx.get());
     unsigned long long hmx = 0;
     readback(&hmx, mx.get(), sizeof(hmx), s);
     need_scratch = 2ull * hmx > (uint64_t)kBlockSlots;
     scratch_len = G.nK;
   }
+  const Lists G0 = G;  // the full lists (version 0)
 
   const size_t smem = ((sizeof(Shared) + 15) & ~size_t(15)) + (size_t)kBlockSlots * 2 * sizeof(uint32_t);
   auto kern = peel_kernel<kWing>;
@@ -1432,7 +1679,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   int grid = sm_count() * per_sm;
   // A single instance may run on fewer CTAs: its barriers and grid-stride phases then span
   // fewer CTAs, which shortens light rounds.
-  int64_t cap = parts && parts->base.size() > 1 ? 0 : tune.max_ctas;
+  int64_t cap = batch ? 0 : tune.max_ctas;
   if (const char* e = getenv("PB_PEEL_CTAS")) cap = atoll(e);  // diagnostic hook
   if (cap > 0) grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, cap));
 
@@ -1441,8 +1688,9 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     gscratch.alloc((size_t)grid * (size_t)scratch_len, s);
     PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
   }
+  DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + (int64_t)pbase.size() + 1, s);
   Work W{};
-  W.D = out;
+  W.D = two_phase ? snap.get() : out;
   W.cnt = cnt.get();
   W.state = state.get();
   W.in_near = in_near.get();
@@ -1468,6 +1716,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   W.gscratch_len = scratch_len;
   W.N = N;
   W.item0 = 0;
+  W.part_out = two_phase ? part.get() : nullptr;
 
   Ctl hctl;
   std::memset(&hctl, 0, sizeof(hctl));
@@ -1480,8 +1729,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   hctl.min_gain = (unsigned)std::max<int64_t>(1 << 16, N / 64);
   // A recorded / captured pipeline runs the peel as one launch without list compaction (the
   // host cannot step in between launches of a CUDA graph); so do per-graph instances.
-  const bool graph_mode = g_recorder != nullptr;
-  if (graph_mode || multi) hctl.min_gain = 0xFFFFFFFFu;
+  if (g_recorder != nullptr || batch) hctl.min_gain = 0xFFFFFFFFu;
   hctl.barrier_timeout_ns = kBarrierTimeoutNs;
   hctl.near_min = (unsigned)tune.near_min;
   hctl.near_div = (unsigned)tune.near_div;
@@ -1500,117 +1748,29 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   DevBuf<unsigned> status(2, s);
-  if (multi) {
-    // CTA shares in proportion to the instances' weights (estimated work): an instance whose
-    // share is at least one CTA gets round(share) CTAs of its own; the light ones are packed,
-    // longest first onto the least-loaded CTA, into the CTAs left over, where they run one
-    // after another.  Each instance keeps its own control block, lists and rounds, so every
-    // graph advances at its own minimum bucket.
-    std::vector<int> ord(ninst);
-    for (int i = 0; i < ninst; ++i) ord[i] = i;
-    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return pweight[a] > pweight[b]; });
-    double wsum = 0;
-    for (double w : pweight) wsum += w;
-    int nheavy = 0;
-    while (nheavy < ninst && pweight[ord[nheavy]] / wsum * grid >= 1.0) ++nheavy;
-    double lw = 0;
-    for (int j = nheavy; j < ninst; ++j) lw += pweight[ord[j]];
-    int light_ctas = 0;
-    if (nheavy < ninst)
-      light_ctas = std::min(ninst - nheavy, std::max(1, (int)std::ceil(lw / wsum * grid)));
-    // Heavy instances share the rest; demote the lightest ones while they outnumber it.
-    while (nheavy > grid - light_ctas) {
-      --nheavy;
-      if (!light_ctas) light_ctas = 1;
-    }
-    if (!nheavy) light_ctas = std::min(grid, ninst);
-    const int hbudget = grid - light_ctas;
-    std::vector<int> ncta(ninst, 0);
-    if (nheavy) {
-      double hw = 0;
-      for (int j = 0; j < nheavy; ++j) hw += pweight[ord[j]];
-      int total = 0;
-      for (int j = 0; j < nheavy; ++j) {
-        ncta[ord[j]] = std::max(1, (int)(pweight[ord[j]] / hw * hbudget));
-        total += ncta[ord[j]];
-      }
-      for (int j = 0; total < hbudget; j = (j + 1) % nheavy, ++total) ++ncta[ord[j]];
-      while (total > hbudget) {  // some instance has more than one CTA here (hbudget >= nheavy)
-        int k = ord[0];
-        for (int j = 1; j < nheavy; ++j)
-          if (ncta[ord[j]] > ncta[k]) k = ord[j];
-        --ncta[k];
-        --total;
-      }
-    }
-    const int nlight = ninst - nheavy;
-    // Instance order of the launch: heavy ones (own CTA ranges), then each light CTA's list.
-    std::vector<int> inst_of;           // launch slot -> instance
-    std::vector<uint32_t> first, cnt, cbeg(grid, 0), cend(grid, 0);
-    uint32_t cta = 0;
-    for (int j = 0; j < nheavy; ++j) {
-      const int i = ord[j];
-      for (int c = 0; c < ncta[i]; ++c) {
-        cbeg[cta + c] = (uint32_t)inst_of.size();
-        cend[cta + c] = (uint32_t)inst_of.size() + 1;
-      }
-      inst_of.push_back(i);
-      first.push_back(cta);
-      cnt.push_back((uint32_t)ncta[i]);
-      cta += (uint32_t)ncta[i];
-    }
-    if (nlight) {
-      std::vector<std::vector<int>> bins(light_ctas);
-      std::vector<double> load(light_ctas, 0.0);
-      for (int j = nheavy; j < ninst; ++j) {
-        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        bins[b].push_back(ord[j]);
-        load[b] += pweight[ord[j]];
-      }
-      for (int b = 0; b < light_ctas; ++b, ++cta) {
-        cbeg[cta] = (uint32_t)inst_of.size();
-        for (int i : bins[b]) {
-          inst_of.push_back(i);
-          first.push_back(cta);
-          cnt.push_back(1u);
-        }
-        cend[cta] = (uint32_t)inst_of.size();
-      }
-    }
+
+  // One cooperative launch of independent instances with CTA shares by weight (no compaction
+  // pauses: every instance runs to its end).  per_slot may adjust each launch slot's Work.
+  auto launch_instances = [&](const std::vector<Work>& wproto, const std::vector<Ctl>& cproto,
+                              const std::vector<double>& weights, const Lists* levels_dev,
+                              const std::function<void(Work&, uint32_t)>& per_slot) {
+    std::vector<int> inst_of;
+    std::vector<uint32_t> first, ncta, cbeg, cend;
+    assign_ctas(weights, grid, inst_of, first, ncta, cbeg, cend);
     const int n_slots = (int)inst_of.size();
-    std::vector<Work> ws(n_slots, W);
-    std::vector<Ctl> hctls(n_slots, hctl);
+    std::vector<Work> ws(n_slots);
+    std::vector<Ctl> hctls(n_slots);
     for (int q = 0; q < n_slots; ++q) {
-      const int i = inst_of[q];
-      const int64_t b = pbase[i], n = psize[i];
-      Work& x = ws[q];
-      x.alist[0] = alist0.get() + b;
-      x.alist[1] = alist1.get() + b;
-      x.near = nearl.get() + b;
-      x.fsmall[0] = fs0.get() + b;
-      x.fsmall[1] = fs1.get() + b;
-      x.fbig[0] = fb0.get() + b;
-      x.fbig[1] = fb1.get() + b;
-      x.fchunks[0] = fc0.get() + b;
-      x.fchunks[1] = fc1.get() + b;
-      x.uprefix = upre.get() + b + i;
-      x.fhuge[0] = fh0.get() + b;
-      x.fhuge[1] = fh1.get() + b;
-      x.tlist[0] = tl0.get() + b;
-      x.tlist[1] = tl1.get() + b;
-      x.N = n;
-      x.item0 = (uint32_t)b;
-      Ctl& c = hctls[q];
-      c.alive = (unsigned)n;
-      c.alen[0] = (unsigned)n;
-      c.alive_at_compact = (unsigned)n;
+      ws[q] = wproto[inst_of[q]];
+      hctls[q] = cproto[inst_of[q]];
+      if (per_slot) per_slot(ws[q], ncta[q]);
     }
     DevBuf<Ctl> ctls(n_slots, s);
     DevBuf<Work> dws(n_slots, s);
     DevBuf<uint32_t> meta(2 * (size_t)n_slots + 2 * (size_t)grid, s);
     std::vector<uint32_t> hmeta;
     hmeta.insert(hmeta.end(), first.begin(), first.end());
-    hmeta.insert(hmeta.end(), cnt.begin(), cnt.end());
+    hmeta.insert(hmeta.end(), ncta.begin(), ncta.end());
     hmeta.insert(hmeta.end(), cbeg.begin(), cbeg.end());
     hmeta.insert(hmeta.end(), cend.begin(), cend.end());
     const void* src_c = hctls.data();
@@ -1633,13 +1793,15 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     Instances I{dws.get(), meta.get(), meta.get() + n_slots, meta.get() + 2 * n_slots,
                 meta.get() + 2 * n_slots + grid, (uint32_t)n_slots};
     Ctl* cp = ctls.get();
-    void* args[] = {&G, &I, &cp, &cls};
+    Lists Gk = G0;
+    const Lists* lv = levels_dev;
+    void* args[] = {&Gk, &lv, &I, &cp, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
     if (g_launch_counter) ++*g_launch_counter;
     PB_LAUNCH(ctl_status_kernel, 1, 32, 0, s, cp, (unsigned)n_slots, status.get());
     if (capturing()) {
       PB_CUDA_TRY(cudaMemcpyAsync(g_recorder->status, status.get(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-      return res;
+      return;
     }
     PB_CUDA_TRY(cudaMemcpyAsync(hctls.data(), cp, sizeof(Ctl) * n_slots, cudaMemcpyDeviceToHost, s));
     PB_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1647,11 +1809,66 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
       PB_REQUIRE(!(c.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
       PB_REQUIRE(c.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
       PB_REQUIRE(c.alive == 0, PB_ECUDA, "peeling: an instance stopped with unpeeled items");
-      res.rounds = std::max<int64_t>(res.rounds, (int64_t)c.rounds);
+      res.rounds += (int64_t)c.rounds;
+      res.fine_rounds_max = std::max<int64_t>(res.fine_rounds_max, (int64_t)c.rounds);
       res.work += (int64_t)c.work;
     }
+  };
+
+  if (batch) {
+    const int ninst = (int)pbase.size();
+    std::vector<Work> ws(ninst, W);
+    std::vector<Ctl> cs(ninst, hctl);
+    for (int i = 0; i < ninst; ++i) {
+      const int64_t b = pbase[i], n = psize[i];
+      Work& x = ws[i];
+      x.alist[0] = alist0.get() + b;
+      x.alist[1] = alist1.get() + b;
+      x.near = nearl.get() + b;
+      x.fsmall[0] = fs0.get() + b;
+      x.fsmall[1] = fs1.get() + b;
+      x.fbig[0] = fb0.get() + b;
+      x.fbig[1] = fb1.get() + b;
+      x.fchunks[0] = fc0.get() + b;
+      x.fchunks[1] = fc1.get() + b;
+      x.uprefix = upre.get() + b + i;
+      x.fhuge[0] = fh0.get() + b;
+      x.fhuge[1] = fh1.get() + b;
+      x.tlist[0] = tl0.get() + b;
+      x.tlist[1] = tl1.get() + b;
+      x.N = n;
+      x.item0 = (uint32_t)b;
+      Ctl& c = cs[i];
+      c.alive = (unsigned)n;
+      c.alen[0] = (unsigned)n;
+      c.alive_at_compact = (unsigned)n;
+    }
+    launch_instances(ws, cs, pweight, nullptr, nullptr);
+    res.rounds = res.fine_rounds_max;  // a batch reports the rounds of its longest graph
+    res.fine_rounds_max = 0;
     return res;
   }
+
+  if (two_phase) {
+    // Coarse pass: partitions of equal estimated work, about parts_per_cta per CTA (or
+    // parts_total in all).
+    DevBuf<unsigned long long> wtot(1, s);
+    DevBuf<unsigned> ctot(1, s);
+    PB_CUDA_TRY(cudaMemsetAsync(wtot.get(), 0, sizeof(unsigned long long), s));
+    PB_CUDA_TRY(cudaMemsetAsync(ctot.get(), 0, sizeof(unsigned), s));
+    PB_LAUNCH(part_stats_kernel<kWing>, grid_for(N), 256, 0, s, G, cls, (const uint32_t*)nullptr, N, ctot.get(),
+              wtot.get());
+    unsigned long long total_w = 0;
+    readback(&total_w, wtot.get(), sizeof(total_w), s);
+    const double nparts_target = std::max(1.0, parts_total > 0 ? (double)parts_total : parts_per_cta * grid);
+    hctl.range_mode = 1;
+    hctl.part_target = std::max<unsigned long long>(1, (unsigned long long)((double)total_w / nparts_target));
+  }
+
+  // Single instance over the whole grid: launch, and between launches compact the lists to
+  // their live entries (every version is kept for the fine pass of a two-phase peel).
+  std::vector<Lists> levels{G0};
+  std::vector<unsigned> level_from{0};  // version j holds every item of partitions >= level_from[j]
   DevBuf<Work> dW(1, s);
   DevBuf<Ctl> ctl(1, s);
   if (capturing()) {
@@ -1669,9 +1886,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   }
   Instances I1{dW.get(), nullptr, nullptr, nullptr, nullptr, 1u};
   Ctl* ctl_ptr = ctl.get();
+  const Lists* no_levels = nullptr;
   int launches = 0;
   if (capturing()) {
-    void* args[] = {&G, &I1, &ctl_ptr, &cls};
+    void* args[] = {&G, &no_levels, &I1, &ctl_ptr, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
     if (g_launch_counter) ++*g_launch_counter;
     // {err, alive} of the control block into the recorder's status slot (pinned).
@@ -1680,7 +1898,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     return res;
   }
   while (true) {
-    void* args[] = {&G, &I1, &ctl_ptr, &cls};
+    void* args[] = {&G, &no_levels, &I1, &ctl_ptr, &cls};
     PB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kPT), args, smem, s));
     if (g_launch_counter) ++*g_launch_counter;
     ++launches;
@@ -1694,38 +1912,152 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     if (kWing) {
       compact_side<true>(liveK, G.offK, G.edgK, G.eidK, state.get(), true, s);
       compact_side<true>(liveC, G.offC, G.edgC, G.eidC, state.get(), true, s);
-      G.offK = liveK.off[liveK.cur].get();
-      G.edgK = liveK.nbr[liveK.cur].get();
-      G.eidK = liveK.eid[liveK.cur].get();
-      G.offC = liveC.off[liveC.cur].get();
-      G.edgC = liveC.nbr[liveC.cur].get();
-      G.eidC = liveC.eid[liveC.cur].get();
+      G.offK = liveK.ver.back()->off.get();
+      G.edgK = liveK.ver.back()->nbr.get();
+      G.eidK = liveK.ver.back()->eid.get();
+      G.offC = liveC.ver.back()->off.get();
+      G.edgC = liveC.ver.back()->nbr.get();
+      G.eidC = liveC.ver.back()->eid.get();
     } else {
       compact_side<false>(liveC, G.offC, G.edgC, nullptr, state.get(), false, s);
-      G.offC = liveC.off[liveC.cur].get();
-      G.edgC = liveC.nbr[liveC.cur].get();
+      G.offC = liveC.ver.back()->off.get();
+      G.edgC = liveC.ver.back()->nbr.get();
     }
-    refresh_work();
+    refresh_work(G);
+    if (two_phase) {
+      // Partitions not opened yet (npart and later) have all their items in the new version.
+      levels.push_back(G);
+      level_from.push_back(hctl.npart);
+    }
     const unsigned alive = hctl.alive;
     PB_CUDA_TRY(cudaMemcpyAsync(&ctl.get()->alive_at_compact, &alive, sizeof(unsigned), cudaMemcpyHostToDevice, s));
   }
   res.rounds = (int64_t)hctl.rounds;
   res.work = (int64_t)hctl.work;
-  if (const char* tr = getenv("PB_TRACE")) {
-    if (*tr && *tr != '0')
-      fprintf(stderr,
-              "[pb] peel %s: rounds %llu launches %d advances %llu | ms advance %.1f F %.1f P %.1f U %.1f | "
-              "near scanned %llu touched %llu items small %llu big %llu huge %llu work %llu\n",
-              kWing ? "wing" : "tip", hctl.rounds, launches, hctl.advances, hctl.phase_ns[0] / 1e6,
-              hctl.phase_ns[1] / 1e6, hctl.phase_ns[2] / 1e6, hctl.phase_ns[3] / 1e6, hctl.scanned,
-              hctl.touched_total, hctl.n_small, hctl.n_big, hctl.n_huge, hctl.work);
-    if (*tr && *tr != '0')
-      for (int b = 0; b < 42; ++b)
-        if (hctl.pbin_rounds[b])
-          fprintf(stderr, "[pb]   P rounds with est work in [2^%d, 2^%d): %llu rounds, %.1f ms, est %.3g (%.3g/s)\n",
-                  b ? b - 1 : 0, b, hctl.pbin_rounds[b], hctl.pbin_ns[b] / 1e6, (double)hctl.pbin_est[b],
-                  hctl.pbin_ns[b] ? hctl.pbin_est[b] / (hctl.pbin_ns[b] / 1e9) : 0.0);
+  const bool trace = [] {
+    const char* tr = getenv("PB_TRACE");
+    return tr && *tr && *tr != '0';
+  }();
+  if (trace) {
+    fprintf(stderr,
+            "[pb] peel %s%s: rounds %llu launches %d advances %llu | ms advance %.1f F %.1f P %.1f U %.1f | "
+            "near scanned %llu touched %llu items small %llu big %llu huge %llu work %llu\n",
+            kWing ? "wing" : "tip", two_phase ? " (coarse pass)" : "", hctl.rounds, launches, hctl.advances,
+            hctl.phase_ns[0] / 1e6, hctl.phase_ns[1] / 1e6, hctl.phase_ns[2] / 1e6, hctl.phase_ns[3] / 1e6,
+            hctl.scanned, hctl.touched_total, hctl.n_small, hctl.n_big, hctl.n_huge, hctl.work);
+    for (int b = 0; b < 42; ++b)
+      if (hctl.pbin_rounds[b])
+        fprintf(stderr, "[pb]   P rounds with est work in [2^%d, 2^%d): %llu rounds, %.1f ms, est %.3g (%.3g/s)\n",
+                b ? b - 1 : 0, b, hctl.pbin_rounds[b], hctl.pbin_ns[b] / 1e6, (double)hctl.pbin_est[b],
+                hctl.pbin_ns[b] ? hctl.pbin_est[b] / (hctl.pbin_ns[b] / 1e9) : 0.0);
   }
+  if (!two_phase) return res;
+
+  // ---- fine pass: one instance per partition, all in one launch ----------------------------
+  res.coarse_rounds = res.rounds;
+  const unsigned nparts = hctl.npart;
+  PB_REQUIRE(nparts >= 1, PB_ECUDA, "two-phase peel: the coarse pass opened no partition");
+  // Items sorted by partition (stable: ascending ids inside a partition).
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < nparts) ++bits;
+  DevBuf<uint32_t> pkeys(N, s), pkeys2(N, s), perm(N, s), perm2(N, s);
+  PB_CUDA_TRY(cudaMemcpyAsync(pkeys.get(), part.get(), sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, s));
+  PB_LAUNCH(iota_kernel, grid_for(N), 256, 0, s, perm.get(), N);
+  const bool alt = radix_sort_pairs_u32(pkeys.get(), perm.get(), pkeys2.get(), perm2.get(), N, 0, bits, s);
+  const uint32_t* items = alt ? perm2.get() : perm.get();
+  DevBuf<unsigned> pcnt(nparts, s);
+  DevBuf<unsigned long long> pwork(nparts, s);
+  PB_CUDA_TRY(cudaMemsetAsync(pcnt.get(), 0, sizeof(unsigned) * nparts, s));
+  PB_CUDA_TRY(cudaMemsetAsync(pwork.get(), 0, sizeof(unsigned long long) * nparts, s));
+  PB_LAUNCH(part_stats_kernel<kWing>, grid_for(N), 256, 0, s, G0, cls, (const uint32_t*)part.get(), N, pcnt.get(),
+            pwork.get());
+  std::vector<unsigned> hcnt(nparts);
+  std::vector<unsigned long long> hwork(nparts);
+  PB_CUDA_TRY(cudaMemcpyAsync(hcnt.data(), pcnt.get(), sizeof(unsigned) * nparts, cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaMemcpyAsync(hwork.data(), pwork.get(), sizeof(unsigned long long) * nparts, cudaMemcpyDeviceToHost, s));
+  PB_CUDA_TRY(cudaStreamSynchronize(s));
+  // Fresh per-item state: every partition starts from the counts its items had when it opened.
+  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, (const int64_t*)snap.get(), N, out, cnt.get(), state.get(),
+            in_near.get(), touched.get());
+  DevBuf<Lists> dlevels(levels.size(), s);
+  PB_CUDA_TRY(cudaMemcpyAsync(dlevels.get(), levels.data(), sizeof(Lists) * levels.size(), cudaMemcpyHostToDevice, s));
+  Ctl c0;
+  std::memset(&c0, 0, sizeof(c0));
+  c0.nm[0] = c0.nm[1] = kInf;
+  c0.k_lo = kInf;
+  c0.min_gain = 0xFFFFFFFFu;
+  c0.barrier_timeout_ns = hctl.barrier_timeout_ns;
+  c0.near_min = hctl.near_min;
+  c0.near_div = hctl.near_div;
+  std::vector<Work> ws;
+  std::vector<Ctl> cs;
+  std::vector<double> weights;
+  int64_t b = 0;
+  for (unsigned p = 0; p < nparts; ++p) {
+    const int64_t n = hcnt[p];
+    if (n == 0) continue;
+    Work x = W;
+    x.D = out;
+    x.part_out = nullptr;
+    x.items = items;
+    x.part = part.get();
+    x.my_part = p;
+    unsigned lv = 0;
+    for (unsigned j = 0; j < level_from.size(); ++j)
+      if (level_from[j] <= p) lv = j;
+    x.level = lv;
+    x.alist[0] = alist0.get() + b;
+    x.alist[1] = alist1.get() + b;
+    x.near = nearl.get() + b;
+    x.fsmall[0] = fs0.get() + b;
+    x.fsmall[1] = fs1.get() + b;
+    x.fbig[0] = fb0.get() + b;
+    x.fbig[1] = fb1.get() + b;
+    x.fchunks[0] = fc0.get() + b;
+    x.fchunks[1] = fc1.get() + b;
+    x.fhuge[0] = fh0.get() + b;
+    x.fhuge[1] = fh1.get() + b;
+    x.tlist[0] = tl0.get() + b;
+    x.tlist[1] = tl1.get() + b;
+    x.N = n;
+    x.item0 = (uint32_t)b;
+    ws.push_back(x);
+    Ctl c = c0;
+    c.alive = (unsigned)n;
+    c.alen[0] = (unsigned)n;
+    c.alive_at_compact = (unsigned)n;
+    cs.push_back(c);
+    weights.push_back(std::max(1.0, (double)hwork[p]));
+    b += n;
+  }
+  PB_REQUIRE(b == N, PB_ECUDA, "two-phase peel: partition sizes do not add up");
+  // Unit prefixes: N + 1 slots per instance (n + 1 each).
+  DevBuf<uint32_t> upre2(N + (int64_t)ws.size() + 1, s);
+  for (size_t i = 0; i < ws.size(); ++i) ws[i].uprefix = upre2.get() + ws[i].item0 + i;
+  const int64_t coarse_work = res.work;
+  res.rounds = 0;
+  res.work = 0;
+  // Grid-shared counters (grid-level items) must be per instance here, since partitions share
+  // item ids: instances with a CTA range of their own get one slice each while the 256 MB
+  // budget lasts; the others never take the grid-level path.
+  const int64_t slices = std::max<int64_t>(1, (int64_t(256) << 20) / (4 * gstride));
+  std::vector<std::unique_ptr<DevBuf<uint32_t>>> gsl;
+  auto per_slot = [&](Work& x, uint32_t ncta) {
+    x.gshared = nullptr;
+    x.ngroups = 1;
+    if (ncta >= 2 && (int64_t)gsl.size() < slices) {
+      gsl.push_back(std::make_unique<DevBuf<uint32_t>>((size_t)gstride, s));
+      PB_CUDA_TRY(cudaMemsetAsync(gsl.back()->get(), 0, gsl.back()->bytes(), s));
+      x.gshared = gsl.back()->get();
+    }
+  };
+  launch_instances(ws, cs, weights, dlevels.get(), per_slot);
+  res.work += coarse_work;
+  res.parts = (int64_t)ws.size();
+  if (trace)
+    fprintf(stderr, "[pb] peel %s fine pass: %zu partitions, %d list versions, %lld rounds, longest %lld\n",
+            kWing ? "wing" : "tip", ws.size(), (int)levels.size(), (long long)res.rounds,
+            (long long)res.fine_rounds_max);
   return res;
 }
 

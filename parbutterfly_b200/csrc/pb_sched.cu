@@ -1,6 +1,7 @@
-// Learned scheduler, peeling side: the work-unit setting of a peel call (which items run on a
-// warp, how a round's CTA-level work is cut into units, which items take the whole grid) is
-// picked by the cost model from call-level features.  Candidates are a fixed grid of
+// Learned scheduler, peeling side: the setting of a peel call (how the exact rounds are batched
+// into partitions of the two-phase schedule, how a round's CTA-level work is cut into units,
+// which items take the whole grid, how many CTAs run) is picked by the cost model from
+// call-level features.  Candidates are a fixed grid of
 // PeelTuning values per peel kind; candidate 0 is the plain path's setting.  The counting side
 // (per-item aggregation modes) lives with the aggregator in pb_count.cu.
 #include <cmath>
@@ -39,9 +40,12 @@ __global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, uns
 constexpr float kPeelMargin = 0.2016f;  // log2(1.15)
 constexpr int64_t kUnits[3] = {4, 2, 8};
 constexpr int64_t kChunk[2] = {512, 2048};
-constexpr int64_t kTipSmall[2] = {512, 256};
 constexpr int64_t kTipHuge[4] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) << 15, int64_t(1) << 40};
 constexpr int kCtaDiv[4] = {1, 2, 4, 8};
+// Peel-round batching: 0 runs one exact round at a time over the whole GPU; p > 0 batches the
+// rounds into about p partitions per CTA (the two-phase schedule).
+constexpr double kWingPpc[6] = {0, 0.5, 1, 2, 4, 8};
+constexpr double kTipPpc[3] = {0, 1, 4};
 
 }  // namespace
 
@@ -50,19 +54,23 @@ int peel_candidates(bool wing) { return wing ? kWingCandidates : kTipCandidates;
 PeelTuning peel_candidate(bool wing, int c, int resident_ctas) {
   PeelTuning t = plain_peel_tuning(wing);
   int div = 1;
+  double ppc = 0;
   if (wing) {
-    // c = units * 2 + chunk on the full grid; c = 0 is the plain setting.  (Fewer CTAs make the
-    // wing peel of a 2^24-edge graph 1.2-1.8x slower, while small graphs suggest the opposite to
-    // a model trained on them, so the wing grid keeps every CTA.)
+    // c = (ppc * 3 + units) * 2 + chunk on the full grid; c = 0 is the plain setting.  (Fewer
+    // CTAs make the one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while small
+    // graphs suggest the opposite to a model trained on them, so the wing grid keeps every CTA.)
     t.chunk_work = kChunk[c % 2];
     t.units_per_cta = kUnits[(c / 2) % 3];
+    ppc = kWingPpc[(c / 6) % 6];
   } else {
-    // c = (small * 4 + huge) * 4 + cta divisor; c = 0 is the plain setting.
+    // c = (ppc * 4 + huge) * 4 + cta divisor; c = 0 is the plain setting.
     div = kCtaDiv[c % 4];
     t.huge_work = kTipHuge[(c / 4) % 4];
-    t.small_work = kTipSmall[(c / 16) % 2];
+    ppc = kTipPpc[(c / 16) % 3];
   }
   t.max_ctas = div > 1 ? std::max(1, resident_ctas / div) : 0;
+  t.two_phase = ppc > 0;
+  t.parts_per_cta = ppc;
   return t;
 }
 
@@ -101,10 +109,15 @@ void peel_call_features(const pb_graph& g, int use_v, bool wing, const int64_t* 
 void peel_row(const float* call_f, bool wing, int c, float* row) {
   const PeelTuning t = peel_candidate(wing, c, 1 << 20);
   for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
-  row[12] = (float)std::log2((double)t.small_work);
-  row[13] = wing ? (float)std::log2((double)t.units_per_cta) : (float)std::log2((double)std::min<int64_t>(t.huge_work, int64_t(1) << 20));
-  row[14] = wing ? (float)std::log2((double)t.chunk_work) : 0.f;
-  row[15] = t.max_ctas > 0 ? (float)std::log2((double)((1 << 20) / t.max_ctas)) : 0.f;  // log2 of the CTA divisor
+  if (wing) {
+    row[12] = (float)std::log2((double)t.units_per_cta);
+    row[13] = (float)std::log2((double)t.chunk_work);
+  } else {
+    row[12] = t.max_ctas > 0 ? (float)std::log2((double)((1 << 20) / t.max_ctas)) : 0.f;  // log2 of the CTA divisor
+    row[13] = (float)std::log2((double)std::min<int64_t>(t.huge_work, int64_t(1) << 20));
+  }
+  row[14] = 0.f;
+  row[15] = (float)std::log2(1.0 + 4.0 * (t.two_phase ? t.parts_per_cta : 0.0));
 }
 
 int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {

@@ -5,8 +5,10 @@ workloads (other seeds and sizes): bipartite R-MAT with three skews, Zipf-endpoi
 uniform graphs.  With tracing in explore mode the plain path logs
   - count: one row per block-aggregator item of every count call (VERT and EDGE, HASH),
     with a random valid aggregation mode per item (target log2 SM cycles of the item);
-  - peel:  one row per tip / wing peel call, sweeping the setting grid (target log2 ms of the
-    call); two larger graphs are traced for tip peeling only.
+  - peel:  one row per tip / wing peel call, sweeping the setting grid (round batching of the
+    two-phase schedule, work units, grid-level thresholds, CTA count; target log2 ms of the
+    call); larger graphs are traced for tip peeling only, and for wing peeling over the
+    round-batching settings only.
 Both MLPs are then trained on the GPU (tensor-core forward / backward, Adam) and saved.
 
     python -m parbutterfly_b200.sched_train --out sched.bin [--quick]
@@ -54,8 +56,15 @@ def make(kind, args, seed) -> BipartiteGraph:
     return BipartiteGraph.uniform(*args, seed)
 
 
-def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=32, log=print,
-            tip_graphs=TIP_GRAPHS):
+# Larger graphs traced for wing peeling with the plain work units and every round batching.
+WING_GRAPHS = [
+    ("rmat", (18, 16, 1 << 22, 0.55, 0.15, 0.15, 0.15), 7301),
+    ("rmat", (19, 17, 1 << 23, 0.45, 0.25, 0.15, 0.15), 7302),
+]
+
+
+def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=48, log=print,
+            tip_graphs=TIP_GRAPHS, wing_graphs=WING_GRAPHS):
     """Explore-mode traces: returns (Xc, yc, Xp, yp)."""
     pb.trace_clear(ctx)
     pb.trace_set(ctx, "explore", seed=1)
@@ -86,6 +95,15 @@ def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS,
                 pb.peel(dg, c)
             dg.close()
             log(f"[sched_train] tip traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
+        for spec in wing_graphs:
+            t0 = time.perf_counter()
+            dg = ctx.upload(make(*spec))
+            ce = pb.count_e(dg, "BATCHS", "ADEG")
+            for b in range(6):  # every round batching with the plain work units: candidates 0, 6, ..., 30
+                pb.trace_set(ctx, "explore", seed=6 * b)  # the sweep position of the next peel call
+                pb.peel_e(dg, ce)
+            dg.close()
+            log(f"[sched_train] wing traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
     finally:
         pb.trace_set(ctx, "off")
     Xc, yc = pb.trace_rows(ctx, pb.SchedModel.COUNT)
@@ -111,10 +129,10 @@ def main():
     ap.add_argument("--quick", action="store_true", help="fewer graphs and peel settings")
     a = ap.parse_args()
     ctx = pb.Context(a.device)
-    cg, pg, ps, tg = COUNT_GRAPHS, PEEL_GRAPHS, 32, TIP_GRAPHS
+    cg, pg, ps, tg, wg = COUNT_GRAPHS, PEEL_GRAPHS, 48, TIP_GRAPHS, WING_GRAPHS
     if a.quick:
-        cg, pg, ps, tg = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16, []
-    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps, tip_graphs=tg)
+        cg, pg, ps, tg, wg = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16, [], []
+    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps, tip_graphs=tg, wing_graphs=wg)
     m = train(ctx, Xc, yc, Xp, yp)
     m.save(a.out)
     print(f"[sched_train] saved {a.out}")
