@@ -292,6 +292,8 @@ constexpr uint32_t kLocalUnits = 2048;  // rounds with at most this many CTA-lev
 struct Shared {
   uint32_t incl[kPT];
   uint32_t sb[kPT];
+  uint32_t len[kPT];
+  uint32_t cursor;
   uint32_t scan[32];
   unsigned long long red[32];
   uint32_t item;
@@ -343,29 +345,40 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* smem, 
   return incl;
 }
 
-// Same iteration by the whole CTA.
+// Same iteration by the whole CTA.  Each chunk of kPT first-level positions has its second-level
+// ranges cut into pieces of at most kPiece entries; warps claim pieces from a shared-memory
+// counter, locate a piece's position once (binary search over the chunk's inclusive piece
+// counts) and walk it with 32 lanes, so consecutive lanes read consecutive entries and no
+// per-entry search is needed.
+constexpr uint32_t kPiece = 128;
+
 template <class First, class F>
 __device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f) {
-  const uint32_t tid = threadIdx.x;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
   for (uint32_t j0 = b; j0 < e; j0 += kPT) {
     const uint32_t j = j0 + tid;
     uint32_t L = 0, sb = 0;
     if (j < e) first(j, L, sb);
     uint32_t T;
-    const uint32_t incl = block_incl_scan(L, S.scan, T);
+    const uint32_t incl = block_incl_scan((L + kPiece - 1) / kPiece, S.scan, T);
     S.incl[tid] = incl;
     S.sb[tid] = sb;
+    S.len[tid] = L;
+    if (tid == 0) S.cursor = 0;
     __syncthreads();
-    for (uint32_t t0 = 0; t0 < T; t0 += kPT) {
-      const uint32_t t = t0 + tid;
-      if (t < T) {
-        uint32_t lo = 0;
+    while (true) {
+      uint32_t p = 0;
+      if (lane == 0) p = atomicAdd(&S.cursor, 1u);
+      p = __shfl_sync(0xffffffffu, p, 0);
+      if (p >= T) break;
+      uint32_t lo = 0;
 #pragma unroll
-        for (uint32_t step = kPT / 2; step > 0; step >>= 1)
-          if (S.incl[lo + step - 1] <= t) lo += step;
-        const uint32_t ex = lo ? S.incl[lo - 1] : 0u;
-        f(j0 + lo, S.sb[lo] + (t - ex));
-      }
+      for (uint32_t step = kPT / 2; step > 0; step >>= 1)
+        if (S.incl[lo + step - 1] <= p) lo += step;
+      const uint32_t k0 = (p - (lo ? S.incl[lo - 1] : 0u)) * kPiece;
+      const uint32_t kend = min(k0 + kPiece, S.len[lo]);
+      const uint32_t sbj = S.sb[lo];
+      for (uint32_t k = k0 + lane; k < kend; k += 32) f(j0 + lo, sbj + k);
     }
     __syncthreads();
   }

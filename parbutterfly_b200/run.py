@@ -20,6 +20,8 @@ GRAPHS = {
     "rmat20": lambda: BipartiteGraph.rmat(20, 18, 1 << 24, 0.55, 0.15, 0.15, 0.15, 2),
     "rmat15": lambda: BipartiteGraph.rmat(15, 13, 1 << 19, 0.55, 0.15, 0.15, 0.15, 2),
     "rmat14": lambda: BipartiteGraph.rmat(14, 12, 1 << 18, 0.55, 0.15, 0.15, 0.15, 2),
+    "plaw10m": lambda: BipartiteGraph.powerlaw_u(100_000, 1_000_000, 10_000_000, 2.0, 100_000, 3),
+    "c3": lambda: workload("c3"),
     "c1": lambda: workload("c1"),
 }
 
@@ -32,6 +34,7 @@ def main(argv=None):
     ap.add_argument("--count-type", default="HASH")
     ap.add_argument("--rank-type", default="ACOCORE")
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--peel-parts", type=int, default=0, help="pb_opts.peel_parts of the peel calls")
     a = ap.parse_args(argv)
     if a.case == "mlp-train":
         import numpy as np
@@ -64,17 +67,21 @@ def main(argv=None):
                 s = ctx.stats()
                 print(f"count-edge w_rank={s['w_rank']} agg_ms={s['ms_agg_kernel']:.2f} total={int(e.sum()) // 4}")
                 if a.case == "peel-edge":
-                    pb.peel_e(dg, e)
+                    pb.peel_e(dg, e, peel_parts=a.peel_parts)
                     s = ctx.stats()
-                    print(f"peel-edge ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']}")
+                    print(f"peel-edge ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']} "
+                          f"parts={s['peel_parts']} coarse_rounds={s['peel_coarse_rounds']} "
+                          f"longest_part_rounds={s['peel_fine_rounds_max']}")
             elif a.case in ("count-vert", "peel-vert"):
                 c = pb.count(dg, a.count_type, a.rank_type)
                 s = ctx.stats()
                 print(f"count-vert w_rank={s['w_rank']} agg_ms={s['ms_agg_kernel']:.2f} total={int(c.sum()) // 2}")
                 if a.case == "peel-vert":
-                    pb.peel(dg, c)
+                    pb.peel(dg, c, peel_parts=a.peel_parts)
                     s = ctx.stats()
-                    print(f"peel-vert ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']}")
+                    print(f"peel-vert ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} work={s['peel_work']} "
+                          f"parts={s['peel_parts']} coarse_rounds={s['peel_coarse_rounds']} "
+                          f"longest_part_rounds={s['peel_fine_rounds_max']}")
             else:
                 t = pb.count_total(dg, a.count_type, a.rank_type)
                 s = ctx.stats()
