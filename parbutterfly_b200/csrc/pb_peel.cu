@@ -301,10 +301,14 @@ struct Shared {
   uint32_t uprefix[kLocalUnits + 1];
 };
 
+// A second-level position with this bit set walks the probe set instead (the reverse direction of
+// a wing intersection); list positions stay below 2^31 (2m <= 2^32).
+constexpr uint32_t kRevFlag = 0x80000000u;
+
 // Flattened two-level iteration by one warp: first(j, L, sb) gives the second-level range
 // [sb, sb + L) of first-level position j in [b, e); f(j, q) is called once per pair.
 template <class First, class F>
-__device__ __forceinline__ void warp_iter(uint32_t b, uint32_t e, First&& first, F&& f) {
+__device__ __forceinline__ void warp_iter(uint32_t b, uint32_t e, First&& first, F&& f, const uint32_t* __restrict__ arr) {
   const unsigned lane = lane_id();
   for (uint32_t j0 = b; j0 < e; j0 += 32) {
     const uint32_t j = j0 + lane;
@@ -323,7 +327,10 @@ __device__ __forceinline__ void warp_iter(uint32_t b, uint32_t e, First&& first,
       }
       const uint32_t ex = __shfl_sync(0xffffffffu, excl, lo);
       const uint32_t s = __shfl_sync(0xffffffffu, sb, lo);
-      if (t < T) f(j0 + lo, s + (t - ex));
+      if (t < T) {
+        const uint32_t q = s + (t - ex);
+        f(j0 + lo, q, arr[q & ~kRevFlag]);
+      }
     }
   }
 }
@@ -353,7 +360,8 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* smem, 
 constexpr uint32_t kPiece = 128;
 
 template <class First, class F>
-__device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f) {
+__device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f,
+                                           const uint32_t* __restrict__ arr) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u;
   for (uint32_t j0 = b; j0 < e; j0 += kPT) {
     const uint32_t j = j0 + tid;
@@ -377,8 +385,19 @@ __device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, Fi
         if (S.incl[lo + step - 1] <= p) lo += step;
       const uint32_t k0 = (p - (lo ? S.incl[lo - 1] : 0u)) * kPiece;
       const uint32_t kend = min(k0 + kPiece, S.len[lo]);
-      const uint32_t sbj = S.sb[lo];
-      for (uint32_t k = k0 + lane; k < kend; k += 32) f(j0 + lo, sbj + k);
+      const uint32_t sbj = S.sb[lo], base = sbj & ~kRevFlag;
+      // A piece is 4 x 32 entries: every lane issues its 4 loads before it uses any of them.
+      uint32_t x[kPiece / 32];
+#pragma unroll
+      for (uint32_t r = 0; r < kPiece / 32; ++r) {
+        const uint32_t k = k0 + lane + 32 * r;
+        x[r] = k < kend ? arr[base + k] : 0u;
+      }
+#pragma unroll
+      for (uint32_t r = 0; r < kPiece / 32; ++r) {
+        const uint32_t k = k0 + lane + 32 * r;
+        if (k < kend) f(j0 + lo, sbj + k, x[r]);
+      }
     }
     __syncthreads();
   }
@@ -388,7 +407,7 @@ __device__ __forceinline__ void block_iter(uint32_t b, uint32_t e, Shared& S, Fi
 // pair of [b, e)); every CTA of the grid takes one slice of a huge item.
 template <class First, class F>
 __device__ __forceinline__ void block_iter_range(uint32_t b, uint32_t e, Shared& S, First&& first, F&& f,
-                                                 uint64_t lo, uint64_t hi) {
+                                                 uint64_t lo, uint64_t hi, const uint32_t* __restrict__ arr) {
   const uint32_t tid = threadIdx.x;
   uint64_t base = 0;
   for (uint32_t j0 = b; j0 < e && base < hi; j0 += kPT) {
@@ -411,7 +430,8 @@ __device__ __forceinline__ void block_iter_range(uint32_t b, uint32_t e, Shared&
         for (uint32_t step = kPT / 2; step > 0; step >>= 1)
           if (S.incl[lo2 + step - 1] <= t) lo2 += step;
         const uint32_t ex = lo2 ? S.incl[lo2 - 1] : 0u;
-        f(j0 + lo2, S.sb[lo2] + (t - ex));
+        const uint32_t q = S.sb[lo2] + (t - ex);
+        f(j0 + lo2, q, arr[q & ~kRevFlag]);
       }
     }
     __syncthreads();
@@ -479,10 +499,10 @@ __device__ void tip_item_warp(const Lists& G, const Work& W, Ctl* ctl, unsigned 
               sb = G.offC[v];
               L = G.offC[v + 1] - sb;
             },
-            [&](uint32_t, uint32_t q) {
-              const uint32_t u2 = G.edgC[q];
+            [&](uint32_t, uint32_t, uint32_t u2) {
               if (u2 != u) t_add(keys, vals, mask, u2, ctl);
-            });
+            },
+            G.edgC);
   __syncwarp();
   for (uint32_t s = lane; s < tsize; s += 32) {
     const uint32_t k = keys[s];
@@ -511,12 +531,11 @@ __device__ void tip_item_block(const Lists& G, const Work& W, Ctl* ctl, unsigned
     sb = G.offC[v];
     L = G.offC[v + 1] - sb;
   };
-  block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-    const uint32_t u2 = G.edgC[q];
+  block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
     if (u2 == u) return;
     if (hash) t_add(keys, vals, mask, u2, ctl);
     else atomicAdd(&gcnt[u2], 1u);
-  });
+  }, G.edgC);
   __syncthreads();
   if (hash) {
     for (uint32_t s = threadIdx.x; s < tsize; s += kPT) {
@@ -526,12 +545,11 @@ __device__ void tip_item_block(const Lists& G, const Work& W, Ctl* ctl, unsigned
       if (w >= 2) dec(W, ctl, par, k, w * (w - 1) / 2);
     }
   } else {
-    block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-      const uint32_t u2 = G.edgC[q];
+    block_iter(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
       if (u2 == u) return;
       const int64_t w = atomicExch(&gcnt[u2], 0u);
       if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
-    });
+    }, G.edgC);
   }
   if (threadIdx.x == 0) work += (unsigned long long)wk;
   __syncthreads();
@@ -542,7 +560,6 @@ __device__ void tip_item_block(const Lists& G, const Work& W, Ctl* ctl, unsigned
 // (u2, edge e2), second level N(u2) (v2, edge e3), probe v2 -> e4.
 // Orientation B (walk from u): probe set N(v) (count-side vertex -> edge), first level N(u)
 // (v2, e4), second level N(v2) (u2, e3), probe u2 -> e2.  Both find the same butterflies.
-constexpr uint32_t kRevFlag = 0x80000000u;  // list positions stay below 2^31 (2m <= 2^32)
 
 // Binary-searching a list of length dbig for each of dsmall keys beats scanning it.
 __device__ __forceinline__ bool reverse_cheaper(uint32_t dsmall, uint32_t dbig) {
@@ -635,15 +652,19 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     if (j != acc.j) { flush(); acc.j = j; }
     acc.acc += 1;
   };
+  // Second-level entries (and the probe set walked in the reverse direction) come from one list
+  // array per orientation: N(u2) / N(u) in the count side's lists when walking from v, N(v2) /
+  // N(v) in the centre side's lists when walking from u.
+  const uint32_t* arr = E.from_v ? G.edgK : G.edgC;
   auto run = [&](uint32_t b, uint32_t e, auto&& first, auto&& f) {
     if (kLevel == LV_WARP) {
-      warp_iter(b, e, first, f);
+      warp_iter(b, e, first, f, arr);
     } else if (kLevel == LV_BLOCK) {
-      block_iter(b, e, *S, first, f);
+      block_iter(b, e, *S, first, f, arr);
     } else {
       const uint64_t T = block_total(b, e, *S, first);
       const uint64_t lo = T * vblock() / vgrid(), hi = T * (vblock() + 1) / vgrid();
-      block_iter_range(b, e, *S, first, f, lo, hi);
+      block_iter_range(b, e, *S, first, f, lo, hi, arr);
     }
   };
   if (E.from_v) {
@@ -654,11 +675,10 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       if (reverse_cheaper(psize, d2)) { sb = pb | kRevFlag; L = psize; }
       else { sb = b2; L = d2; }
     };
-    auto f = [&](uint32_t p, uint32_t q) {
+    auto f = [&](uint32_t p, uint32_t q, uint32_t v2) {  // v2 = G.edgK[q without the flag]
       ++my_work;
       if (q & kRevFlag) {  // walk N(u), binary-search N(u2)
         const uint32_t pos = q & ~kRevFlag;
-        const uint32_t v2 = G.edgK[pos];
         if (v2 == E.v) return;
         const uint32_t e4 = G.eidK[pos];
         if (skip_edge(W, e4, E.e1)) return;
@@ -671,7 +691,6 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
         found(p, e3, e4);
         return;
       }
-      const uint32_t v2 = G.edgK[q];
       if (v2 == E.v) return;
       uint32_t e4;
       if (!probe(v2, e4)) return;  // most probes miss: test the table before any global read
@@ -689,11 +708,10 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       if (reverse_cheaper(psize, d2)) { sb = pb | kRevFlag; L = psize; }
       else { sb = b2; L = d2; }
     };
-    auto f = [&](uint32_t q, uint32_t p3) {
+    auto f = [&](uint32_t q, uint32_t p3, uint32_t u2) {  // u2 = G.edgC[p3 without the flag]
       ++my_work;
       if (p3 & kRevFlag) {  // walk N(v), binary-search N(v2)
         const uint32_t pos = p3 & ~kRevFlag;
-        const uint32_t u2 = G.edgC[pos];
         if (u2 == E.u) return;
         const uint32_t e2 = G.eidC[pos];
         if (skip_edge(W, e2, E.e1)) return;
@@ -706,7 +724,6 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
         found(q, e2, e3);
         return;
       }
-      const uint32_t u2 = G.edgC[p3];
       if (u2 == E.u) return;
       uint32_t e2;
       if (!probe(u2, e2)) return;
@@ -738,17 +755,15 @@ __device__ bool tip_item_grid(const Lists& G, const Work& W, Ctl* ctl, unsigned 
   const uint64_t T = (uint64_t)G.wk[u] + (G.offK[u + 1] - G.offK[u]);
   const uint64_t lo = T * vblock() / vgrid(), hi = T * (vblock() + 1) / vgrid();
   uint32_t* cnt = W.gshared;
-  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-    const uint32_t u2 = G.edgC[q];
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
     if (u2 != u) atomicAdd(&cnt[u2], 1u);
-  }, lo, hi);
+  }, lo, hi, G.edgC);
   if (!grid_barrier(ctl)) return false;
-  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-    const uint32_t u2 = G.edgC[q];
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
     if (u2 == u) return;
     const int64_t w = atomicExch(&cnt[u2], 0u);
     if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
-  }, lo, hi);
+  }, lo, hi, G.edgC);
   if (vblock() == 0 && threadIdx.x == 0) work += T;
   return grid_barrier(ctl);
 }
@@ -765,17 +780,15 @@ __device__ bool tip_item_group(const Lists& G, const Work& W, Ctl* ctl, unsigned
   };
   const uint64_t T = (uint64_t)G.wk[u] + (G.offK[u + 1] - G.offK[u]);
   const uint64_t lo = T * lb / gs, hi = T * (lb + 1) / gs;
-  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-    const uint32_t u2 = G.edgC[q];
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
     if (u2 != u) atomicAdd(&cnt[u2], 1u);
-  }, lo, hi);
+  }, lo, hi, G.edgC);
   if (!group_barrier(ctl, slot, gs)) return false;
-  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t q) {
-    const uint32_t u2 = G.edgC[q];
+  block_iter_range(G.offK[u], G.offK[u + 1], S, first, [&](uint32_t, uint32_t, uint32_t u2) {
     if (u2 == u) return;
     const int64_t w = atomicExch(&cnt[u2], 0u);
     if (w >= 2) dec(W, ctl, par, u2, w * (w - 1) / 2);
-  }, lo, hi);
+  }, lo, hi, G.edgC);
   if (lb == 0 && threadIdx.x == 0) work += T;
   return true;
 }
