@@ -833,6 +833,9 @@ pb_status pb_peel_vert_batch(pb_ctx* ctx, const pb_graph* const* gs, int32_t k, 
     ctx->stats.ms_peel = T.ms(0, 1);
     ctx->stats.peel_rounds = pr.rounds;
     ctx->stats.peel_work = pr.work;
+    ctx->stats.peel_parts = pr.parts;
+    ctx->stats.peel_coarse_rounds = pr.coarse_rounds;
+    ctx->stats.peel_fine_rounds_max = pr.fine_rounds_max;
     ctx->stats.sched_meas = ctx->stats.ms_peel;
     log_peel_trace(ctx, row, ctx->stats.ms_peel);
   });

@@ -80,6 +80,9 @@ struct Ctl {
   unsigned long long part_target;
   unsigned long long whist[66];    // estimated work per log2 distance bin
   unsigned long long wsub[256];    // estimated work per linear sub-bin of the chosen octave
+  // Wing items per probe structure (warp table, CTA table, dense markers, grid) and their probes;
+  // probes that walked the probe set against a binary search (the reverse direction).
+  unsigned long long mode_items[4], mode_work[4], rev_work;
 };
 constexpr unsigned kMaxGroups = 32;
 
@@ -637,7 +640,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     return true;
   };
   PosAcc acc;
-  unsigned long long my_work = 0;
+  unsigned long long my_work = 0, my_rev = 0;
   auto flush = [&]() {
     if (acc.j != kEmpty && acc.acc) dec(W, ctl, par, E.from_v ? G.eidC[acc.j] : G.eidK[acc.j], acc.acc);
     acc.acc = 0;
@@ -678,6 +681,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     auto f = [&](uint32_t p, uint32_t q, uint32_t v2) {  // v2 = G.edgK[q without the flag]
       ++my_work;
       if (q & kRevFlag) {  // walk N(u), binary-search N(u2)
+        ++my_rev;
         const uint32_t pos = q & ~kRevFlag;
         if (v2 == E.v) return;
         const uint32_t e4 = G.eidK[pos];
@@ -711,6 +715,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     auto f = [&](uint32_t q, uint32_t p3, uint32_t u2) {  // u2 = G.edgC[p3 without the flag]
       ++my_work;
       if (p3 & kRevFlag) {  // walk N(v), binary-search N(v2)
+        ++my_rev;
         const uint32_t pos = p3 & ~kRevFlag;
         if (u2 == E.u) return;
         const uint32_t e2 = G.eidC[pos];
@@ -736,6 +741,16 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   }
   flush();
   work += my_work;
+  {
+    const int mode = kLevel == LV_WARP ? 0 : (kLevel == LV_GRID ? 3 : (hash ? 1 : 2));
+    const unsigned long long w = warp_sum((unsigned long long)my_work);
+    const unsigned long long rw = warp_sum((unsigned long long)my_rev);
+    if (lane_id() == 0) {
+      if (w) atomicAdd(&ctl->mode_work[mode], w);
+      if (rw) atomicAdd(&ctl->rev_work, rw);
+    }
+    if (rank == 0) atomicAdd(&ctl->mode_items[mode], 1ull);
+  }
   if (!sync()) return false;
   if (!hash) {  // clear the dense markers
     for (uint32_t p = pb + rank; p < pe; p += gsize) mark[E.from_v ? G.edgK[p] : G.edgC[p]] = 0;
@@ -1500,6 +1515,20 @@ __global__ void part_stats_kernel(Lists G, Classify cls, const uint32_t* __restr
   }
 }
 
+// gid[x] = i for the items x in [base[i], base[i + 1]) (one CTA per range).
+__global__ void range_ids_kernel(const uint32_t* __restrict__ base, uint32_t n, const uint32_t* unused, uint32_t* gid) {
+  const uint32_t i = blockIdx.x;
+  if (i >= n) return;
+  for (uint32_t x = base[i] + threadIdx.x; x < base[i + 1]; x += blockDim.x) gid[x] = i;
+}
+
+// key[x] = pbase[gid[x]] + part[x]: graph-major global partition ids of a batch.
+__global__ void global_part_kernel(const uint32_t* __restrict__ gid, const uint32_t* __restrict__ part,
+                                   const uint32_t* __restrict__ pbase, int64_t N, uint32_t* key) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < N; x += (int64_t)gridDim.x * blockDim.x)
+    key[x] = pbase[gid[x]] + part[x];
+}
+
 // Splits `grid` CTAs among instances by weight: an instance whose share is at least one CTA
 // gets a CTA range of its own (its barriers span only that range); the light ones are packed,
 // longest first onto the least-loaded CTA, into the CTAs left over, where they run one after
@@ -1612,6 +1641,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     two_phase_req = parts_per_cta > 0;
   }
   const bool two_phase = !batch && two_phase_req && g_recorder == nullptr;
+  const bool two_phase_batch = batch && two_phase_req && g_recorder == nullptr;
 
   DevBuf<int64_t> cnt(N, s);
   DevBuf<uint32_t> eti, iota, center_of, touched(N, s), alist0(N, s), alist1(N, s), nearl(N, s);
@@ -1645,12 +1675,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   liveK.keep_all = liveC.keep_all = two_phase;
   DevBuf<int64_t> snap;  // two-phase: every item's count when its partition opens
   DevBuf<uint32_t> part;
-  if (two_phase) {
+  if (two_phase || two_phase_batch) {
     snap.alloc(N, s);
     part.alloc(N, s);
   }
-  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, two_phase ? snap.get() : out, cnt.get(), state.get(),
-            in_near.get(), touched.get());
+  PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, counts, N, (two_phase || two_phase_batch) ? snap.get() : out,
+            cnt.get(), state.get(), in_near.get(), touched.get());
   // Work estimates of the lists a version holds: neighbour-degree sums (wing) or two-hop wedges
   // (tip).
   std::vector<std::unique_ptr<DevBuf<int64_t>>> work_bufs;
@@ -1716,7 +1746,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   }
   DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + (int64_t)pbase.size() + 1, s);
   Work W{};
-  W.D = two_phase ? snap.get() : out;
+  W.D = (two_phase || two_phase_batch) ? snap.get() : out;
   W.cnt = cnt.get();
   W.state = state.get();
   W.in_near = in_near.get();
@@ -1779,7 +1809,8 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   // pauses: every instance runs to its end).  per_slot may adjust each launch slot's Work.
   auto launch_instances = [&](const std::vector<Work>& wproto, const std::vector<Ctl>& cproto,
                               const std::vector<double>& weights, const Lists* levels_dev,
-                              const std::function<void(Work&, uint32_t)>& per_slot) {
+                              const std::function<void(Work&, uint32_t)>& per_slot,
+                              std::vector<Ctl>* inst_out = nullptr) {
     std::vector<int> inst_of;
     std::vector<uint32_t> first, ncta, cbeg, cend;
     assign_ctas(weights, grid, inst_of, first, ncta, cbeg, cend);
@@ -1831,13 +1862,16 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     }
     PB_CUDA_TRY(cudaMemcpyAsync(hctls.data(), cp, sizeof(Ctl) * n_slots, cudaMemcpyDeviceToHost, s));
     PB_CUDA_TRY(cudaStreamSynchronize(s));
-    for (const Ctl& c : hctls) {
+    if (inst_out) inst_out->assign(wproto.size(), Ctl{});
+    for (int q = 0; q < n_slots; ++q) {
+      const Ctl& c = hctls[q];
       PB_REQUIRE(!(c.err & ERR_TIMEOUT), PB_ETIMEOUT, "peeling: a grid barrier wait ran out of time");
       PB_REQUIRE(c.err == 0, PB_ECUDA, "peeling: a table invariant was violated");
       PB_REQUIRE(c.alive == 0, PB_ECUDA, "peeling: an instance stopped with unpeeled items");
       res.rounds += (int64_t)c.rounds;
       res.fine_rounds_max = std::max<int64_t>(res.fine_rounds_max, (int64_t)c.rounds);
       res.work += (int64_t)c.work;
+      if (inst_out) (*inst_out)[inst_of[q]] = c;
     }
   };
 
@@ -1869,9 +1903,141 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
       c.alen[0] = (unsigned)n;
       c.alive_at_compact = (unsigned)n;
     }
-    launch_instances(ws, cs, pweight, nullptr, nullptr);
-    res.rounds = res.fine_rounds_max;  // a batch reports the rounds of its longest graph
+    if (!two_phase_batch) {
+      launch_instances(ws, cs, pweight, nullptr, nullptr);
+      res.rounds = res.fine_rounds_max;  // a batch reports the rounds of its longest graph
+      res.fine_rounds_max = 0;
+      return res;
+    }
+    // Two-phase schedule per graph: a coarse pass with one range-mode instance per graph (about
+    // parts_per_cta partitions per CTA, split by the graphs' work), then one fine instance per
+    // (graph, partition).  Partition ids are local to a graph: items of different graphs never
+    // meet in a list.
+    DevBuf<uint32_t> gid(N, s);
+    DevBuf<uint32_t> dbase(ninst + 1, s);
+    std::vector<uint32_t> hb(ninst + 1);
+    for (int i = 0; i < ninst; ++i) hb[i] = (uint32_t)pbase[i];
+    hb[ninst] = (uint32_t)(pbase[ninst - 1] + psize[ninst - 1]);
+    PB_CUDA_TRY(cudaMemcpyAsync(dbase.get(), hb.data(), sizeof(uint32_t) * (ninst + 1), cudaMemcpyHostToDevice, s));
+    PB_LAUNCH(range_ids_kernel, ninst, 256, 0, s, dbase.get(), (uint32_t)ninst, (const uint32_t*)nullptr, gid.get());
+    DevBuf<unsigned> icnt(ninst, s);
+    DevBuf<unsigned long long> iwork(ninst, s);
+    PB_CUDA_TRY(cudaMemsetAsync(icnt.get(), 0, sizeof(unsigned) * ninst, s));
+    PB_CUDA_TRY(cudaMemsetAsync(iwork.get(), 0, sizeof(unsigned long long) * ninst, s));
+    PB_LAUNCH(part_stats_kernel<kWing>, grid_for(N), 256, 0, s, G, cls, (const uint32_t*)gid.get(), N, icnt.get(),
+              iwork.get());
+    std::vector<unsigned long long> hiw(ninst);
+    PB_CUDA_TRY(cudaMemcpyAsync(hiw.data(), iwork.get(), sizeof(unsigned long long) * ninst, cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    double wsum = 0;
+    for (unsigned long long w : hiw) wsum += (double)w;
+    const double want = std::max(1.0, parts_total > 0 ? (double)parts_total : parts_per_cta * grid);
+    for (int i = 0; i < ninst; ++i) {
+      const double parts_i = std::max(1.0, std::round(want * (double)hiw[i] / std::max(1.0, wsum)));
+      cs[i].range_mode = 1;
+      cs[i].part_target = std::max<unsigned long long>(1, (unsigned long long)((double)hiw[i] / parts_i));
+      ws[i].part_out = part.get();
+    }
+    std::vector<Ctl> coarse;
+    launch_instances(ws, cs, pweight, nullptr, nullptr, &coarse);
+    res.coarse_rounds = res.fine_rounds_max;
+    res.rounds = 0;
     res.fine_rounds_max = 0;
+    // Global partition keys (graph-major) and the fine instances in that order.
+    std::vector<uint32_t> pb0(ninst + 1, 0);
+    for (int i = 0; i < ninst; ++i) pb0[i + 1] = pb0[i] + std::max(1u, coarse[i].npart);
+    const uint32_t ntot = pb0[ninst];
+    DevBuf<uint32_t> dpb(ninst + 1, s), key(N, s);
+    PB_CUDA_TRY(cudaMemcpyAsync(dpb.get(), pb0.data(), sizeof(uint32_t) * (ninst + 1), cudaMemcpyHostToDevice, s));
+    PB_LAUNCH(global_part_kernel, grid_for(N), 256, 0, s, (const uint32_t*)gid.get(), (const uint32_t*)part.get(),
+              (const uint32_t*)dpb.get(), N, key.get());
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < ntot) ++bits;
+    DevBuf<uint32_t> key2(N, s), perm(N, s), perm2(N, s);
+    PB_LAUNCH(iota_kernel, grid_for(N), 256, 0, s, perm.get(), N);
+    const bool alt = radix_sort_pairs_u32(key.get(), perm.get(), key2.get(), perm2.get(), N, 0, bits, s);
+    const uint32_t* items = alt ? perm2.get() : perm.get();
+    // key still holds each item's global partition (radix_sort_pairs_u32 sorts into key / key2).
+    PB_LAUNCH(global_part_kernel, grid_for(N), 256, 0, s, (const uint32_t*)gid.get(), (const uint32_t*)part.get(),
+              (const uint32_t*)dpb.get(), N, key2.get());
+    DevBuf<unsigned> pcnt(ntot, s);
+    DevBuf<unsigned long long> pwork(ntot, s);
+    PB_CUDA_TRY(cudaMemsetAsync(pcnt.get(), 0, sizeof(unsigned) * ntot, s));
+    PB_CUDA_TRY(cudaMemsetAsync(pwork.get(), 0, sizeof(unsigned long long) * ntot, s));
+    PB_LAUNCH(part_stats_kernel<kWing>, grid_for(N), 256, 0, s, G, cls, (const uint32_t*)key2.get(), N, pcnt.get(),
+              pwork.get());
+    std::vector<unsigned> hcnt(ntot);
+    std::vector<unsigned long long> hwork(ntot);
+    PB_CUDA_TRY(cudaMemcpyAsync(hcnt.data(), pcnt.get(), sizeof(unsigned) * ntot, cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaMemcpyAsync(hwork.data(), pwork.get(), sizeof(unsigned long long) * ntot, cudaMemcpyDeviceToHost, s));
+    PB_CUDA_TRY(cudaStreamSynchronize(s));
+    PB_LAUNCH(peel_init_kernel, grid_for(N), 256, 0, s, (const int64_t*)snap.get(), N, out, cnt.get(), state.get(),
+              in_near.get(), touched.get());
+    std::vector<Work> fws;
+    std::vector<Ctl> fcs;
+    std::vector<double> fw;
+    std::vector<int> graph_of;
+    int64_t b = 0;
+    for (int i = 0; i < ninst; ++i) {
+      for (uint32_t p = 0; p + pb0[i] < pb0[i + 1]; ++p) {
+        const int64_t n = hcnt[pb0[i] + p];
+        if (n == 0) continue;
+        Work x = ws[i];
+        x.D = out;
+        x.part_out = nullptr;
+        x.items = items;
+        x.part = part.get();
+        x.my_part = p;
+        x.alist[0] = alist0.get() + b;
+        x.alist[1] = alist1.get() + b;
+        x.near = nearl.get() + b;
+        x.fsmall[0] = fs0.get() + b;
+        x.fsmall[1] = fs1.get() + b;
+        x.fbig[0] = fb0.get() + b;
+        x.fbig[1] = fb1.get() + b;
+        x.fchunks[0] = fc0.get() + b;
+        x.fchunks[1] = fc1.get() + b;
+        x.fhuge[0] = fh0.get() + b;
+        x.fhuge[1] = fh1.get() + b;
+        x.tlist[0] = tl0.get() + b;
+        x.tlist[1] = tl1.get() + b;
+        x.N = n;
+        x.item0 = (uint32_t)b;
+        fws.push_back(x);
+        Ctl c = hctl;
+        c.alive = (unsigned)n;
+        c.alen[0] = (unsigned)n;
+        c.alive_at_compact = (unsigned)n;
+        fcs.push_back(c);
+        fw.push_back(std::max(1.0, (double)hwork[pb0[i] + p]));
+        graph_of.push_back(i);
+        b += n;
+      }
+    }
+    PB_REQUIRE(b == N, PB_ECUDA, "two-phase peel: partition sizes do not add up");
+    DevBuf<uint32_t> upre2(N + (int64_t)fws.size() + 1, s);
+    for (size_t i = 0; i < fws.size(); ++i) fws[i].uprefix = upre2.get() + fws[i].item0 + i;
+    const int64_t gstride_b = gstride;
+    const int64_t slices = std::max<int64_t>(1, (int64_t(256) << 20) / (4 * gstride_b));
+    std::vector<std::unique_ptr<DevBuf<uint32_t>>> gsl;
+    auto per_slot = [&](Work& x, uint32_t ncta) {
+      x.gshared = nullptr;
+      x.ngroups = 1;
+      if (ncta >= 2 && (int64_t)gsl.size() < slices) {
+        gsl.push_back(std::make_unique<DevBuf<uint32_t>>((size_t)gstride_b, s));
+        PB_CUDA_TRY(cudaMemsetAsync(gsl.back()->get(), 0, gsl.back()->bytes(), s));
+        x.gshared = gsl.back()->get();
+      }
+    };
+    std::vector<Ctl> fine;
+    const int64_t coarse_work = res.work;
+    res.work = 0;
+    launch_instances(fws, fcs, fw, nullptr, per_slot, &fine);
+    std::vector<int64_t> per_graph(ninst, 0);
+    for (size_t q = 0; q < fine.size(); ++q) per_graph[graph_of[q]] += (int64_t)fine[q].rounds;
+    res.rounds = *std::max_element(per_graph.begin(), per_graph.end());  // the longest graph, as above
+    res.work += coarse_work;
+    res.parts = (int64_t)fws.size();
     return res;
   }
 
@@ -1971,6 +2137,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
             kWing ? "wing" : "tip", two_phase ? " (coarse pass)" : "", hctl.rounds, launches, hctl.advances,
             hctl.phase_ns[0] / 1e6, hctl.phase_ns[1] / 1e6, hctl.phase_ns[2] / 1e6, hctl.phase_ns[3] / 1e6,
             hctl.scanned, hctl.touched_total, hctl.n_small, hctl.n_big, hctl.n_huge, hctl.work);
+    if (kWing)
+      fprintf(stderr,
+              "[pb]   wing items / probes: warp %llu / %llu, CTA table %llu / %llu, dense markers %llu / %llu, "
+              "grid %llu / %llu; reverse-direction probes %llu\n",
+              hctl.mode_items[0], hctl.mode_work[0], hctl.mode_items[1], hctl.mode_work[1], hctl.mode_items[2],
+              hctl.mode_work[2], hctl.mode_items[3], hctl.mode_work[3], hctl.rev_work);
     for (int b = 0; b < 42; ++b)
       if (hctl.pbin_rounds[b])
         fprintf(stderr, "[pb]   P rounds with est work in [2^%d, 2^%d): %llu rounds, %.1f ms, est %.3g (%.3g/s)\n",

@@ -89,3 +89,20 @@ def test_two_phase_random_graphs_vs_oracle(ctx):
         dg.close()
         np.testing.assert_array_equal(w, oracle.peel_edge_fast(g, e)[0])
         np.testing.assert_array_equal(t, oracle.peel_vert(g, c)[0])
+
+
+@pytest.mark.parametrize("parts", [16, 500])
+def test_two_phase_batch_of_graphs(ctx, parts):
+    graphs = [BipartiteGraph.batch_member(k) for k in range(24)]
+    dgs = [ctx.upload(g) for g in graphs]
+    try:
+        counts = pb.count_batch(dgs, "BATCHS", "ADEG")
+        plain = pb.peel_batch(dgs, counts)
+        two = pb.peel_batch(dgs, counts, peel_parts=parts)
+        assert ctx.stats()["peel_parts"] >= 1
+        for g, c, a, b in zip(graphs, counts, plain, two):
+            np.testing.assert_array_equal(a, b)
+            np.testing.assert_array_equal(b, oracle.peel_vert(g, c)[0])
+    finally:
+        for dg in dgs:
+            dg.close()
