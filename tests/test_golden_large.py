@@ -7,6 +7,10 @@
   plaw10m : the skewed power-law-degree workload at 1e7 edges: per-vertex counts (largest above
             2^32) and tip numbers (digests).
   c2count : the full benchmark graph (2^24 edges): per-edge counts (digest) and the total.
+  c2wing  : the full benchmark graph's wing numbers (digest), from the oracle's bucket-queue
+            wing peel (oracle/pb_oracle_fast.c, pinned to the reference on every smaller fixture)
+            run on per-edge counts equal to the reference's; the reference's own wing peel of
+            this graph does not finish within hours.
 
 The CPU tests check that the generators still produce the graphs the reference saw; the GPU
 tests compare the CUDA path with the reference's results bit for bit.
@@ -114,6 +118,28 @@ def test_tip_numbers_match_reference(ctx, large, name):
         assert int(c.sum()) // 2 == int(r["use_v_wside_total"][2])
         tip = pb.peel(dg, c)
         _check(tip, r, "peel", name)
+    finally:
+        dg.close()
+
+
+def test_benchmark_wing_record_is_consistent(large):
+    r = _rec(large, "c2wing")
+    assert str(r["graph_sha"]) == str(_rec(large, "c2count")["graph_sha"])
+    rounds, wmax = (int(x) for x in r["rounds_max"])
+    assert rounds == 131618 and int(r["peel_sample"].max()) <= wmax
+
+
+@pytest.mark.gpu
+def test_benchmark_graph_wing_numbers(ctx, large):
+    from parbutterfly_b200 import butterflies as pb
+    r = _rec(large, "c2wing")
+    g = GRAPHS["c2count"]()
+    dg = ctx.upload(g)
+    try:
+        e = pb.count_e(dg, "HASH", "ACOCORE")
+        wing = pb.peel_e(dg, e)
+        assert ctx.stats()["peel_rounds"] == int(r["rounds_max"][0])
+        _check(wing, r, "peel", "c2wing")
     finally:
         dg.close()
 
