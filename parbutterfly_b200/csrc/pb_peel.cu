@@ -603,7 +603,9 @@ enum Level { LV_WARP = 0, LV_BLOCK = 1, LV_GRID = 2 };
 template <int kLevel>
 __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par, const WingEdge& E, uint32_t* keys,
                           uint32_t* vals, uint32_t slots, Shared* S, unsigned long long& work, uint32_t chunk = 0,
-                          uint32_t nchunks = 1) {
+                          uint32_t nchunks = 1, uint32_t chunk_end = 0) {
+  // First-level slice: units [chunk, chunk_end) of nchunks (chunk_end 0: chunk + 1).
+  if (chunk_end == 0) chunk_end = chunk + 1;
   const uint32_t rank = kLevel == LV_WARP ? lane_id() : (kLevel == LV_GRID ? vblock() * kPT + threadIdx.x : threadIdx.x);
   const uint32_t gsize = kLevel == LV_WARP ? 32 : (kLevel == LV_GRID ? vgrid() * kPT : kPT);
   auto sync = [&]() -> bool {
@@ -703,7 +705,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       found(p, e3, e4);
     };
     const uint32_t b1 = G.offC[E.v], d1 = G.offC[E.v + 1] - b1;
-    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * (chunk + 1) / nchunks), first, f);
+    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * chunk_end / nchunks), first, f);
   } else {
     auto first = [&](uint32_t q, uint32_t& L, uint32_t& sb) {
       const uint32_t v2 = G.edgK[q];
@@ -737,7 +739,7 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
       found(q, e2, e3);
     };
     const uint32_t b1 = G.offK[E.u], d1 = G.offK[E.u + 1] - b1;
-    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * (chunk + 1) / nchunks), first, f);
+    run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * chunk_end / nchunks), first, f);
   }
   flush();
   work += my_work;
@@ -1184,12 +1186,16 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         else if (!grid_barrier(ctl)) return false;
         const uint32_t* upre = local ? S.uprefix : W.uprefix;
         const unsigned nu = local ? S.uprefix[nb] : *(volatile unsigned*)&ctl->units;
+        // CTAs claim runs of K consecutive units (wing: about a quarter of a CTA's share; tip: one
+        // unit, which is one item); the units of one item inside a run are processed as one
+        // slice, so the item's probe table is built once per run, not once per unit.
+        const unsigned K = kWing ? max(1u, nu / (4u * vgrid())) : 1u;
         while (true) {
-          if (threadIdx.x < 32) {  // warp 0: take a unit, find its item (last prefix <= u), 32-way
+          if (threadIdx.x < 32) {  // warp 0: take a run, find the item of its first unit, 32-way
             unsigned u = 0;
-            if (lane == 0) u = atomicAdd(&ctl->cur_big[par], 1u);
+            if (lane == 0) u = atomicAdd(&ctl->cur_big[par], K);
             u = __shfl_sync(0xffffffffu, u, 0);
-            uint32_t lo = 0, hi = nb;  // answer in [lo, hi)
+            uint32_t lo = 0, hi = nb;  // answer in [lo, hi): the last item whose prefix <= u
             if (u < nu) {
               while (hi - lo > 1) {
                 const uint32_t step = (hi - lo + 31) / 32;
@@ -1207,21 +1213,28 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             }
           }
           __syncthreads();
-          const unsigned u = S.item, q = S.hist[0];
+          const unsigned u0 = S.item, q0 = S.hist[0];
           __syncthreads();
-          if (u >= nu) break;
-          const uint32_t x = W.fbig[par][q];
-          if (W.cnt[x] == 0) continue;  // uniform across the CTA
-          if (kWing) {
-            WingEdge E;
-            E.e1 = x;
-            E.v = G.center_of[x];
-            E.u = G.u_of[x];
-            E.from_v = cls.wing_from_v(G, E.v, E.u);
-            const uint32_t base = upre[q], nch = upre[q + 1] - base;
-            wing_item<LV_BLOCK>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work, u - base, nch);
-          } else {
-            tip_item_block(G, W, ctl, par, x, pool, S, work);
+          if (u0 >= nu) break;
+          const unsigned uend = min(u0 + K, nu);
+          for (unsigned uu = u0, q = q0; uu < uend; ++q) {  // uniform across the CTA
+            const uint32_t base = upre[q], next = upre[q + 1];
+            const uint32_t c1 = min(uend, next);
+            const uint32_t x = W.fbig[par][q];
+            if (W.cnt[x] != 0) {  // no live butterfly contains x: nothing to remove
+              if (kWing) {
+                WingEdge E;
+                E.e1 = x;
+                E.v = G.center_of[x];
+                E.u = G.u_of[x];
+                E.from_v = cls.wing_from_v(G, E.v, E.u);
+                wing_item<LV_BLOCK>(G, W, ctl, par, E, pool, pool + kBlockSlots, kBlockSlots, &S, work, uu - base,
+                                    next - base, c1 - base);
+              } else {
+                tip_item_block(G, W, ctl, par, x, pool, S, work);
+              }
+            }
+            uu = c1;
           }
         }
       }
