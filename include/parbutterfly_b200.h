@@ -158,8 +158,15 @@ pb_status pb_graph_from_device(pb_ctx* ctx, const pb_csr* dev, pb_graph** out);
 pb_status pb_graph_parse_text(pb_ctx* ctx, const char* text, size_t len, pb_graph** out);
 /* The same for a file: read into pinned host memory, parsed on the device. */
 pb_status pb_graph_read_text(pb_ctx* ctx, const char* path, pb_graph** out);
+/* The graph of pb_gen_rmat (same arguments, same graph) generated on the device of ctx, for
+ * sizes whose host generation does not fit host memory (no counterpart in the reference, whose
+ * generators run on the CPU: utils/rMatGraph.C). */
+pb_status pb_gen_rmat_device(pb_ctx* ctx, int32_t log_nv, int32_t log_nu, int64_t m, double a, double b, double c,
+                             double d, uint64_t seed, pb_graph** out);
 pb_status pb_graph_destroy(pb_graph* g);
 pb_status pb_graph_dims(const pb_graph* g, int64_t* nv, int64_t* nu, int64_t* m);
+/* Copies a device graph back to host memory (release with pb_csr_free). */
+pb_status pb_graph_download(const pb_graph* g, pb_csr_owned* out);
 
 /* cmpWedgeCounts (butterfly_utils.h:1080-1086): *use_v = (W_V <= W_U), *num_wedges = min. */
 pb_status pb_cmp_wedge_counts(pb_ctx* ctx, const pb_graph* g, int32_t* use_v, int64_t* num_wedges);

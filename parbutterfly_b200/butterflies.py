@@ -149,6 +149,12 @@ class DeviceGraph:
     def handle(self):
         return self._h
 
+    def download(self) -> BipartiteGraph:
+        """The graph copied back to host memory."""
+        s = _ffi.CSR()
+        self.ctx.check(self.ctx._lib.pb_graph_download(self._h, C.byref(s)), "pb_graph_download")
+        return BipartiteGraph._from_owned(s)
+
 
 def graph_from_text(ctx: Context, data) -> DeviceGraph:
     """readBipartite on the device: `data` is the AdjacencyHypergraph text as bytes (host) or a
@@ -162,6 +168,15 @@ def graph_from_text(ctx: Context, data) -> DeviceGraph:
         torch.cuda.synchronize()
         ctx.check(ctx._lib.pb_graph_parse_text(ctx.handle, data.data_ptr(), data.numel(), C.byref(h)),
                   "pb_graph_parse_text")
+    return DeviceGraph._adopt(ctx, h)
+
+
+def gen_rmat_device(ctx: Context, log_nv: int, log_nu: int, m: int, a: float, b: float, c: float, d: float,
+                    seed: int) -> DeviceGraph:
+    """The graph of BipartiteGraph.rmat (same arguments) generated on the device."""
+    h = C.c_void_p()
+    ctx.check(ctx._lib.pb_gen_rmat_device(ctx.handle, log_nv, log_nu, m, a, b, c, d, seed, C.byref(h)),
+              "pb_gen_rmat_device")
     return DeviceGraph._adopt(ctx, h)
 
 

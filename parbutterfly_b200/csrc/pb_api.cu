@@ -624,6 +624,17 @@ pb_status pb_graph_parse_text(pb_ctx* ctx, const char* text, size_t len, pb_grap
   });
 }
 
+pb_status pb_gen_rmat_device(pb_ctx* ctx, int32_t log_nv, int32_t log_nu, int64_t m, double a, double b, double c,
+                             double d, uint64_t seed, pb_graph** out) {
+  return guarded(ctx, [&] {
+    PB_REQUIRE(out, PB_EINVAL, "null argument");
+    ParsedCSR P;
+    gen_rmat_device(log_nv, log_nu, m, a, b, c, d, seed, P, ctx->stream);
+    const pb_csr cs{P.nv, P.nu, P.m, P.offV.get(), P.edgV.get(), P.offU.get(), P.edgU.get()};
+    upload_graph(ctx, &cs, true, out);  // validated on the device (offsets, ranges, sorted lists)
+  });
+}
+
 pb_status pb_graph_read_text(pb_ctx* ctx, const char* path, pb_graph** out) {
   return guarded(ctx, [&] {
     PB_REQUIRE(path && out, PB_EINVAL, "null argument");
@@ -662,6 +673,35 @@ pb_status pb_graph_destroy(pb_graph* g) {
   delete g;
   cudaSetDevice(prev);
   return PB_OK;
+}
+
+pb_status pb_graph_download(const pb_graph* g, pb_csr_owned* out) {
+  if (!g || !out) return PB_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(g->device);
+  out->nv = g->nv;
+  out->nu = g->nu;
+  out->m = g->m;
+  out->offsetsV = (uint32_t*)malloc(sizeof(uint32_t) * (g->nv + 1));
+  out->offsetsU = (uint32_t*)malloc(sizeof(uint32_t) * (g->nu + 1));
+  out->edgesV = (uint32_t*)malloc(sizeof(uint32_t) * (g->m > 0 ? g->m : 1));
+  out->edgesU = (uint32_t*)malloc(sizeof(uint32_t) * (g->m > 0 ? g->m : 1));
+  pb_status st = PB_OK;
+  if (!out->offsetsV || !out->offsetsU || !out->edgesV || !out->edgesU) {
+    st = PB_ENOMEM;
+  } else {
+    cudaDeviceSynchronize();
+    if (cudaMemcpy(out->offsetsV, g->offV.get(), sizeof(uint32_t) * (g->nv + 1), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(out->offsetsU, g->offU.get(), sizeof(uint32_t) * (g->nu + 1), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        (g->m > 0 && (cudaMemcpy(out->edgesV, g->edgV.get(), sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                      cudaMemcpy(out->edgesU, g->edgU.get(), sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost) != cudaSuccess)))
+      st = PB_ECUDA;
+  }
+  if (st != PB_OK) pb_csr_free(out);
+  cudaSetDevice(prev);
+  return st;
 }
 
 pb_status pb_graph_dims(const pb_graph* g, int64_t* nv, int64_t* nu, int64_t* m) {

@@ -328,6 +328,11 @@ __device__ __forceinline__ void block_wedges(uint32_t b, uint32_t e, const Param
 }
 
 enum Mode : uint32_t { MODE_DENSE = 0, MODE_HASH = 1, MODE_GLOBAL = 2, MODE_HYBRID = 3 };
+// A scheduler mode entry that leaves the item to the plain rule (items too light for the
+// choice to matter are not scored by the learned scheduler).
+constexpr uint8_t kPlainRule = 0xFF;
+// Items with fewer wedges are left to the plain rule when the learned scheduler runs.
+constexpr int64_t kSchedMinWedges = 2048;
 
 __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uint32_t* __restrict__ items,
                                                              const uint32_t* __restrict__ n_items_dev,
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(kBlock) count_block_kernel(Params P, const uin
     const bool tag_i = !(P.adj[b] & 1u);
     const bool need_center = P.per == EDGE || (P.per == VERT && !tag_i);
     Mode mode;
-    if (P.modes) mode = (Mode)(P.modes[q] & 3u);
+    if (P.modes && P.modes[q] != kPlainRule) mode = (Mode)(P.modes[q] & 3u);
     else if (i <= cap_dense && (uint64_t)i <= 4ull * (uint64_t)W) mode = MODE_DENSE;
     else if ((uint64_t)2 * W <= cap_hash) mode = MODE_HASH;
     else if (i <= cap_dense) mode = MODE_DENSE;
@@ -629,6 +634,33 @@ __global__ void sched_choose_kernel(const float* __restrict__ y, const uint8_t* 
   }
 }
 
+// sub[k]: the positions q of block-aggregator items with at least min_w wedges.
+__global__ void heavy_items_kernel(const uint32_t* __restrict__ items, uint32_t n_items,
+                                   const int64_t* __restrict__ wsum, int64_t min_w, uint32_t* sub, uint32_t* n_sub) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = items[q];
+    if (wsum[i + 1] - wsum[i] >= min_w) sub[atomicAdd(n_sub, 1u)] = (uint32_t)q;
+  }
+}
+
+__global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint32_t n,
+                                  uint32_t* dst) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    dst[k] = src[idx[k]];
+}
+
+// Scatters the scored items' modes, predictions and features back to their positions.
+__global__ void scatter_scored_kernel(const uint32_t* __restrict__ sub, uint32_t n, const uint8_t* __restrict__ msub,
+                                      const float* __restrict__ psub, const float* __restrict__ fsub, uint8_t* modes,
+                                      float* pred, float* F) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t q = sub[k];
+    modes[q] = msub[k];
+    pred[q] = psub[k];
+    for (int f = 0; f < kMlpIn; ++f) F[(size_t)q * kMlpIn + f] = fsub[(size_t)k * kMlpIn + f];
+  }
+}
+
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
@@ -750,10 +782,41 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     sCyc.alloc(ni, s);
     sNG.alloc(1, s);
     PB_CUDA_TRY(cudaMemsetAsync(sNG.get(), 0, sizeof(uint32_t), s));
-    PB_LAUNCH(item_features_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 32, 256), sms * 8)), 256, 0, s, P,
-              items.get(), ni, cap_dense, cap_hash, hy_dense, hy_hash, sF.get(), sValid.get());
     const int g1 = std::max(1, std::min(ceil_div(ni, 256), sms * 8));
-    if (sh->model) {
+    // Learned choices score only the items heavy enough for the mode to matter (the rest keep
+    // the plain rule, so the scheduler's own cost stays small); tracing covers every item.
+    if (sh->model && !sh->trace_X) {
+      DevBuf<uint32_t> sub(ni, s), nsub(1, s);
+      PB_CUDA_TRY(cudaMemsetAsync(nsub.get(), 0, sizeof(uint32_t), s));
+      PB_LAUNCH(heavy_items_kernel, g1, 256, 0, s, items.get(), ni, R.wsum.get(), kSchedMinWedges, sub.get(), nsub.get());
+      uint32_t nh = 0;
+      readback(&nh, nsub.get(), sizeof(nh), s);
+      sModes.alloc(ni, s);
+      sPred.alloc(ni, s);
+      PB_CUDA_TRY(cudaMemsetAsync(sModes.get(), kPlainRule, ni, s));
+      PB_CUDA_TRY(cudaMemsetAsync(sPred.get(), 0xFF, sizeof(float) * ni, s));  // NaN: no prediction
+      PB_CUDA_TRY(cudaMemsetAsync(sF.get(), 0, sF.bytes(), s));
+      if (nh > 0) {
+        DevBuf<uint32_t> hitems(nh, s);
+        DevBuf<float> hF((size_t)nh * kMlpIn, s), hPr(nh, s);
+        DevBuf<uint8_t> hValid(nh, s), hModes(nh, s);
+        const int gh = std::max(1, std::min(ceil_div(nh, 256), sms * 8));
+        PB_LAUNCH(gather_u32_kernel, gh, 256, 0, s, items.get(), sub.get(), nh, hitems.get());
+        PB_LAUNCH(item_features_kernel, std::max(1, std::min(ceil_div((int64_t)nh * 32, 256), sms * 8)), 256, 0, s, P,
+                  hitems.get(), nh, cap_dense, cap_hash, hy_dense, hy_hash, hF.get(), hValid.get());
+        DevBuf<float> X((size_t)nh * 3 * kMlpIn, s), y((size_t)nh * 3, s);
+        PB_LAUNCH(sched_candidates_kernel, std::max(1, std::min(ceil_div((int64_t)nh * 3 * kMlpIn, 256), sms * 8)), 256,
+                  0, s, hF.get(), nh, X.get());
+        sh->model->predict_dev(X.get(), (int64_t)nh * 3, y.get(), s);
+        PB_LAUNCH(sched_choose_kernel, gh, 256, 0, s, y.get(), hValid.get(), nh, hModes.get(), hPr.get(), sNG.get());
+        PB_LAUNCH(scatter_scored_kernel, gh, 256, 0, s, sub.get(), nh, hModes.get(), hPr.get(), hF.get(), sModes.get(),
+                  sPred.get(), sF.get());
+      }
+    } else {
+      PB_LAUNCH(item_features_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 32, 256), sms * 8)), 256, 0, s, P,
+                items.get(), ni, cap_dense, cap_hash, hy_dense, hy_hash, sF.get(), sValid.get());
+    }
+    if (sh->model && sh->trace_X) {
       DevBuf<float> X((size_t)ni * 3 * kMlpIn, s), y((size_t)ni * 3, s);
       PB_LAUNCH(sched_candidates_kernel, std::max(1, std::min(ceil_div((int64_t)ni * 3 * kMlpIn, 256), sms * 8)), 256,
                 0, s, sF.get(), ni, X.get());
@@ -772,7 +835,7 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     PB_CUDA_TRY(cudaMemcpyAsync(&ng, sNG.get(), sizeof(ng), cudaMemcpyDeviceToHost, s));
     PB_CUDA_TRY(cudaEventRecord(a1, s));
     PB_CUDA_TRY(cudaEventSynchronize(a1));
-    if (P.modes) need_global = ng > 0;
+    if (P.modes) need_global = ng > 0 || hc[1] > 0;  // unscored items follow the plain rule
     float ms = 0;
     PB_CUDA_TRY(cudaEventElapsedTime(&ms, a0, a1));
     sh->ms = ms;

@@ -99,6 +99,9 @@ struct ParsedCSR {
   DevBuf<uint32_t> offV, edgV, offU, edgU;
 };
 void parse_adjacency_hypergraph(const char* text, size_t len, bool on_device, ParsedCSR& out, cudaStream_t s);
+// The graph of the host R-MAT generator (pb_gen.cpp), generated on the device (pb_gen_dev.cu).
+void gen_rmat_device(int log_nv, int log_nu, int64_t m, double a, double b, double c, double d, uint64_t seed,
+                     ParsedCSR& out, cudaStream_t s);
 
 // Batches (pb_batch.cu): the disjoint union of k graphs, each graph's count side on the union's
 // U side (count with use_v = 1); kbase/ksize locate each graph's count side in the union.

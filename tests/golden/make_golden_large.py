@@ -29,7 +29,12 @@ Records (the reference's flags in brackets):
              reference's own wing numbers on every golden graph and on rmat18; this record is
              the restatement's output, not the reference's (provenance stored with it).
 
-Usage: python tests/golden/make_golden_large.py [--skip-c2] [--c2-wing] [--threads N]
+  c3tip    : (--c3-tip) the skewed power-law-degree workload at full size (|U| = 1e6, |V| = 1e5,
+             m = 1e8, seed 3): per-vertex counts and tip numbers (digests) from the C restatement
+             (64-bit buckets; its counts exceed 2^32, where the reference's 32-bit buckets are not
+             exact), pinned to the reference on plaw10m and every smaller fixture.
+
+Usage: python tests/golden/make_golden_large.py [--skip-c2] [--c2-wing] [--c3-tip] [--threads N]
 """
 import argparse
 import hashlib
@@ -79,10 +84,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-c2", action="store_true")
     ap.add_argument("--c2-wing", action="store_true", help="only add the c2wing record (needs c2count)")
+    ap.add_argument("--c3-tip", action="store_true", help="only add the c3tip record")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     a = ap.parse_args()
     if a.c2_wing:
         c2_wing(a.threads)
+        return
+    if a.c3_tip:
+        c3_tip()
         return
     assert oracle.have_reference(), "build oracle/_ref first (make -C oracle)"
     out = {}
@@ -139,6 +148,29 @@ def c2_wing(threads):
     out["c2wing/rounds_max"] = np.array([rounds, int(wing.max())], dtype=np.int64)
     np.savez_compressed(OUT, **out)
     print(f"c2wing: count {t1 - t0:.1f}s wing {t2 - t1:.1f}s rounds {rounds} max {int(wing.max())}", flush=True)
+
+
+def c3_tip():
+    g = BipartiteGraph.powerlaw_u(100_000, 1_000_000, 100_000_000, 2.0, 100_000, 3)
+    t0 = time.time()
+    c, w_rank = oracle.count(g, "VERT", "ADEG")
+    t1 = time.time()
+    tip, rounds = oracle.peel_vert(g, c)
+    t2 = time.time()
+    with np.load(OUT) as z:
+        out = {k: z[k] for k in z.files}
+    rng = np.random.default_rng(1234)
+    idx = np.sort(rng.choice(c.size, size=SAMPLE, replace=False))
+    out["c3tip/graph_sha"] = np.array(graph_digest(g))
+    out["c3tip/provenance"] = np.array("oracle/pb_oracle.c ranked count (ADEG, VERT) and 64-bit-bucket tip peel")
+    out["c3tip/count_sha"] = np.array(digest(c))
+    out["c3tip/peel_sha"] = np.array(digest(tip))
+    out["c3tip/sample_idx"] = idx.astype(np.int64)
+    out["c3tip/count_sample"] = c[idx]
+    out["c3tip/peel_sample"] = tip[idx]
+    out["c3tip/total_rounds_wrank"] = np.array([int(c.sum()) // 2, rounds, w_rank], dtype=np.int64)
+    np.savez_compressed(OUT, **out)
+    print(f"c3tip: count {t1 - t0:.1f}s tip {t2 - t1:.1f}s rounds {rounds} total {int(c.sum()) // 2}", flush=True)
 
 
 if __name__ == "__main__":
