@@ -8,7 +8,9 @@
 
 Graphs: rmat20 = bipartite R-MAT 2^20 x 2^18, m = 2^24, (.55,.15,.15,.15), seed 2 (the
 benchmark workload); rmat15 = the same generator at 2^15 x 2^13, m = 2^19; rmat14 at
-2^14 x 2^12, m = 2^18; c1 = uniform 4096 x 4096, m = 131072, seed 1.
+2^14 x 2^12, m = 2^18; c1 = uniform 4096 x 4096, m = 131072, seed 1; plaw10m / c3 = the
+power-law-degree workload at 1e7 / 1e8 edges; generated on the device: c5 = bipartite R-MAT
+2^26 x 2^24, m = 1e9, (.57,.19,.19,.05), seed 5, and rmat20d = the benchmark graph.
 """
 import argparse
 import sys
@@ -26,11 +28,19 @@ GRAPHS = {
 }
 
 
+# Graphs generated on the device (pb_gen_rmat_device): the 1e9-edge R-MAT workload does not fit
+# a host generator's memory.
+DEVICE_GRAPHS = {
+    "c5": lambda ctx: pb.gen_rmat_device(ctx, 26, 24, 1_000_000_000, 0.57, 0.19, 0.19, 0.05, 5),
+    "rmat20d": lambda ctx: pb.gen_rmat_device(ctx, 20, 18, 1 << 24, 0.55, 0.15, 0.15, 0.15, 2),
+}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["count-edge", "count-vert", "count-total", "peel-edge", "peel-vert", "mlp-train",
                                      "batch-graph"])
-    ap.add_argument("--graph", default="rmat15", choices=sorted(GRAPHS))
+    ap.add_argument("--graph", default="rmat15", choices=sorted(GRAPHS) + sorted(DEVICE_GRAPHS))
     ap.add_argument("--count-type", default="HASH")
     ap.add_argument("--rank-type", default="ACOCORE")
     ap.add_argument("--repeat", type=int, default=1)
@@ -58,9 +68,14 @@ def main(argv=None):
                 print(f"batch-graph replay ms={ctx.stats()['ms_count']:.1f}")
             bg.close()
         return 0
-    g = GRAPHS[a.graph]()
     with pb.Context(0) as ctx:
-        dg = ctx.upload(g)
+        if a.graph in DEVICE_GRAPHS:
+            import time
+            t0 = time.perf_counter()
+            dg = DEVICE_GRAPHS[a.graph](ctx)
+            print(f"generated on the device: nv={dg.nv} nu={dg.nu} m={dg.m} in {time.perf_counter() - t0:.1f} s")
+        else:
+            dg = ctx.upload(GRAPHS[a.graph]())
         for _ in range(a.repeat):
             if a.case in ("count-edge", "peel-edge"):
                 e = pb.count_e(dg, a.count_type, a.rank_type)
