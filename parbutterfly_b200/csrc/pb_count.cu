@@ -788,7 +788,9 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
     if (sh->model && !sh->trace_X) {
       DevBuf<uint32_t> sub(ni, s), nsub(1, s);
       PB_CUDA_TRY(cudaMemsetAsync(nsub.get(), 0, sizeof(uint32_t), s));
-      PB_LAUNCH(heavy_items_kernel, g1, 256, 0, s, items.get(), ni, R.wsum.get(), kSchedMinWedges, sub.get(), nsub.get());
+      int64_t min_w = kSchedMinWedges;
+      if (const char* ev = getenv("PB_SCHED_MIN_WEDGES")) min_w = atoll(ev);  // test hook: score light items too
+      PB_LAUNCH(heavy_items_kernel, g1, 256, 0, s, items.get(), ni, R.wsum.get(), min_w, sub.get(), nsub.get());
       uint32_t nh = 0;
       readback(&nh, nsub.get(), sizeof(nh), s);
       sModes.alloc(ni, s);
@@ -844,8 +846,16 @@ CountResult count_ranked(const Ranked& R, int per, int64_t* out, const CountConf
   }
   DevBuf<uint32_t> gscratch;
   if (hc[0] > 0) {
-    const int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * blocks_per_sm);
+    int grid = (int)std::min<int64_t>(hc[0], (int64_t)sms * blocks_per_sm);
     if (need_global) {
+      // One dense counter array of n entries per CTA: at very large n (the 1e9-edge R-MAT) the
+      // CTA count is capped so the arrays stay within half of the free device memory (64 GB at
+      // most).
+      size_t free_b = 0, total_b = 0;
+      PB_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+      const size_t budget = std::min<size_t>(free_b / 2, size_t(64) << 30);
+      const size_t per_cta = (size_t)n * sizeof(uint32_t);
+      grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)(budget / per_cta)));
       gscratch.alloc((size_t)grid * (size_t)n, s);
       PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
     }

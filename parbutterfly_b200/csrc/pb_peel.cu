@@ -83,6 +83,7 @@ struct Ctl {
   // Wing items per probe structure (warp table, CTA table, dense markers, grid) and their probes;
   // probes that walked the probe set against a binary search (the reverse direction).
   unsigned long long mode_items[4], mode_work[4], rev_work;
+  unsigned prev_items;  // frontier items of the previous round
 };
 constexpr unsigned kMaxGroups = 32;
 
@@ -817,6 +818,11 @@ struct Classify {
   int64_t huge_work;   // items above this run on the whole grid
   int64_t chunk_work;  // target probes per work unit of a CTA-level wing item
   int64_t units_per_cta;  // work units per CTA a round's CTA-level wing work is cut into
+  // Wing rounds after a round of at least busy_items items (enough to keep every warp busy)
+  // send items up to small_work_busy probes to warps: many independent warp items hide the
+  // latency of their dependent loads better than CTA work units, which synchronise.
+  int64_t small_work_busy;
+  int64_t busy_items;
 
   __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const {
     return G.wk[u] <= kWarpSlots / 2 && G.wk[u] <= small_work;
@@ -1055,6 +1061,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
     // items is the first part of the next round's minimum.
     {
       const unsigned nl = *(volatile unsigned*)&ctl->near_len;
+      const bool busy = (int64_t)*(volatile unsigned*)&ctl->prev_items >= cls.busy_items;
       unsigned long long mn = kInf;
       for (unsigned q = gtid; q < nl; q += gthreads) {
         const uint32_t x = W.near[q];
@@ -1070,7 +1077,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             const bool fv = cv <= cu;
             cost = fv ? cv : cu;
             const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
-            small = cost <= cls.small_work && 2 * psize <= (uint32_t)kWarpSlots;
+            small = cost <= (busy ? cls.small_work_busy : cls.small_work) && 2 * psize <= (uint32_t)kWarpSlots;
             huge = !small && cost > cls.huge_work && W.gshared != nullptr;
           } else {
             cost = G.wk[x];
@@ -1314,6 +1321,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         ctl->n_small += ns;
         ctl->n_big += nb;
         ctl->n_huge += nh;
+        ctl->prev_items = ns + nb + nh;  // read by the next round's phase F after two barriers
       }
     }
     if (!grid_barrier(ctl)) return false;
@@ -1810,10 +1818,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
   if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
-  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
+  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta),
+               std::max(tune.small_work, tune.small_work_busy), 2ll * grid * (kPT / 32)};
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
   if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);
+  if (const char* e = getenv("PB_PEEL_SMALL_WORK_BUSY")) cls.small_work_busy = std::max<int64_t>(cls.small_work, atoll(e));
   if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   DevBuf<unsigned> status(2, s);

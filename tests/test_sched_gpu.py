@@ -17,6 +17,7 @@ def small_items(monkeypatch):
     graphs reach all four aggregation modes."""
     monkeypatch.setenv("PB_COUNT_SMALL_W", "0")
     monkeypatch.setenv("PB_COUNT_SMEM", "16384")
+    monkeypatch.setenv("PB_SCHED_MIN_WEDGES", "0")  # the learned choice scores every item here
 
 
 def _rmat(seed, lv=11, lu=10, m=20000):
