@@ -39,7 +39,7 @@ DEVICE_GRAPHS = {
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["count-edge", "count-vert", "count-total", "peel-edge", "peel-vert", "mlp-train",
-                                     "batch-graph"])
+                                     "batch-graph", "batch-peel"])
     ap.add_argument("--graph", default="rmat15", choices=sorted(GRAPHS) + sorted(DEVICE_GRAPHS))
     ap.add_argument("--count-type", default="HASH")
     ap.add_argument("--rank-type", default="ACOCORE")
@@ -57,6 +57,19 @@ def main(argv=None):
                 mse = m.train(m.COUNT, X, y, epochs=2, batch=8192, lr=3e-3)
                 print(f"mlp-train rows={len(y)} mse={mse:.4f}")
             m.close()
+        return 0
+    if a.case == "batch-peel":
+        gs = [BipartiteGraph.batch_member(k) for k in range(256)]
+        with pb.Context(0) as ctx:
+            dgs = [ctx.upload(g) for g in gs]
+            cs = pb.count_batch(dgs, "BATCHS", "ADEG")
+            print(f"batch-peel count ms={ctx.stats()['ms_count']:.1f}")
+            for _ in range(a.repeat):
+                pb.peel_batch(dgs, cs, peel_parts=a.peel_parts)
+                s = ctx.stats()
+                print(f"batch-peel ms={s['ms_peel']:.1f} rounds={s['peel_rounds']} parts={s['peel_parts']}")
+            for dg in dgs:
+                dg.close()
         return 0
     if a.case == "batch-graph":
         gs = [BipartiteGraph.batch_member(k) for k in range(256)]
