@@ -33,8 +33,8 @@ namespace pb {
 namespace {
 
 constexpr int kPT = 512;
-constexpr int kWarpSlots = 512;    // per-warp table slots (keys + values: 4 KiB)
-constexpr int kBlockSlots = 8192;  // per-CTA table slots (64 KiB), shares memory with warp tables
+constexpr int kWarpSlots = 512;    // per-warp table slots (keys, values, hit counters: 6 KiB)
+constexpr int kBlockSlots = 8192;  // per-CTA table slots (96 KiB), shares memory with warp tables
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kInf = ~0ull;
 constexpr uint8_t ALIVE = 0, ACTIVE = 1, PEELED = 2;
@@ -77,7 +77,11 @@ struct Ctl {
   // unpeeled item is below it.  The bound is chosen so that the window holds about
   // part_target of estimated work.  npart counts the partitions opened so far.
   unsigned range_mode, npart;
-  unsigned long long part_target;
+  unsigned long long part_target;  // base target per partition
+  // Partitions grow past their opening bound (items fall below it while the partition peels):
+  // part_done sums the estimated work actually peeled, part_used the target the partition was
+  // opened with, part_ratio_q (x256, smoothed) their ratio, which scales the next target down.
+  unsigned long long part_done, part_used, part_ratio_q;
   unsigned long long whist[66];    // estimated work per log2 distance bin
   unsigned long long wsub[256];    // estimated work per linear sub-bin of the chosen octave
   // Wing items per probe structure (warp table, CTA table, dense markers, grid) and their probes;
@@ -287,6 +291,18 @@ __device__ __forceinline__ bool t_get(const uint32_t* keys, const uint32_t* vals
     h = (h + 1) & mask;
   }
   return false;
+}
+
+// Slot of key, or kEmpty when absent.
+__device__ __forceinline__ uint32_t t_slot(const uint32_t* keys, uint32_t mask, uint32_t key) {
+  uint32_t h = hslot(key, mask);
+  for (uint32_t probes = 0; probes <= mask; ++probes) {
+    const uint32_t k = keys[h];
+    if (k == key) return h;
+    if (k == kEmpty) return kEmpty;
+    h = (h + 1) & mask;
+  }
+  return kEmpty;
 }
 
 __device__ __forceinline__ uint32_t np2(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
@@ -623,8 +639,14 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   uint32_t* mark = kLevel == LV_GRID ? W.gshared : W.gscratch + (size_t)blockIdx.x * (size_t)W.gscratch_len;
   const uint32_t tsize = hash ? max(64u, np2(2u * psize)) : 0u;
   const uint32_t mask = tsize - 1;
+  // hits[slot]: butterflies found through a probe-set edge, charged to it in one decrement once
+  // the intersections are done (the table area holds keys, edges and hits).
+  uint32_t* hits = vals + slots;
   if (hash)
-    for (uint32_t s = rank; s < tsize; s += gsize) keys[s] = kEmpty;
+    for (uint32_t s = rank; s < tsize; s += gsize) {
+      keys[s] = kEmpty;
+      hits[s] = 0;
+    }
   if (!sync()) return false;
   for (uint32_t p = pb + rank; p < pe; p += gsize) {
     uint32_t key, e;
@@ -635,8 +657,15 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
     else mark[key] = e + 1;
   }
   if (!sync()) return false;
-  auto probe = [&](uint32_t key, uint32_t& e) -> bool {
-    if (hash) return t_get(keys, vals, mask, key, e);
+  // e: the probe-set edge of key; slot: its table slot (kEmpty for the dense markers).
+  auto probe = [&](uint32_t key, uint32_t& e, uint32_t& slot) -> bool {
+    if (hash) {
+      slot = t_slot(keys, mask, key);
+      if (slot == kEmpty) return false;
+      e = vals[slot];
+      return true;
+    }
+    slot = kEmpty;
     const uint32_t x = mark[key];
     if (!x) return false;
     e = x - 1;
@@ -652,9 +681,12 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
   // N(x) and probe the probe-set table, or (when the probe set is much shorter than N(x))
   // walk the probe set and binary-search N(x), which is sorted.  The direction rides in the
   // top bit of the second-level position.
-  auto found = [&](uint32_t j, uint32_t ea, uint32_t eb) {
-    dec(W, ctl, par, ea, 1);
-    dec(W, ctl, par, eb, 1);
+  // One butterfly: e_list (unique to it) loses 1 now; the probe-set edge e_set loses 1 through
+  // its hit counter when it has a table slot; the first-level edge through the accumulator.
+  auto found = [&](uint32_t j, uint32_t e_list, uint32_t e_set, uint32_t slot) {
+    dec(W, ctl, par, e_list, 1);
+    if (slot != kEmpty) atomicAdd(&hits[slot], 1u);
+    else dec(W, ctl, par, e_set, 1);
     if (j != acc.j) { flush(); acc.j = j; }
     acc.acc += 1;
   };
@@ -695,15 +727,15 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
         if (at == hi || G.edgK[at] != v2) return;
         const uint32_t e3 = G.eidK[at];
         if (skip_edge(W, e3, E.e1)) return;
-        found(p, e3, e4);
+        found(p, e3, e4, kEmpty);
         return;
       }
       if (v2 == E.v) return;
-      uint32_t e4;
-      if (!probe(v2, e4)) return;  // most probes miss: test the table before any global read
+      uint32_t e4, slot;
+      if (!probe(v2, e4, slot)) return;  // most probes miss: test the table before any global read
       const uint32_t e3 = G.eidK[q];
       if (skip_edge(W, e3, E.e1) || active_before(W, e4, E.e1)) return;
-      found(p, e3, e4);
+      found(p, e3, e4, slot);
     };
     const uint32_t b1 = G.offC[E.v], d1 = G.offC[E.v + 1] - b1;
     run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * chunk_end / nchunks), first, f);
@@ -729,21 +761,28 @@ __device__ bool wing_item(const Lists& G, const Work& W, Ctl* ctl, unsigned par,
         if (at == hi || G.edgC[at] != u2) return;
         const uint32_t e3 = G.eidC[at];
         if (skip_edge(W, e3, E.e1)) return;
-        found(q, e2, e3);
+        found(q, e3, e2, kEmpty);
         return;
       }
       if (u2 == E.u) return;
-      uint32_t e2;
-      if (!probe(u2, e2)) return;
+      uint32_t e2, slot;
+      if (!probe(u2, e2, slot)) return;
       const uint32_t e3 = G.eidC[p3];
       if (skip_edge(W, e3, E.e1) || active_before(W, e2, E.e1)) return;
-      found(q, e2, e3);
+      found(q, e3, e2, slot);
     };
     const uint32_t b1 = G.offK[E.u], d1 = G.offK[E.u + 1] - b1;
     run(b1 + (uint32_t)((uint64_t)d1 * chunk / nchunks), b1 + (uint32_t)((uint64_t)d1 * chunk_end / nchunks), first, f);
   }
   flush();
   work += my_work;
+  if (hash) {  // the probe-set edges' decrements, one per edge
+    if (!sync()) return false;
+    for (uint32_t s = rank; s < tsize; s += gsize) {
+      const uint32_t h = hits[s];
+      if (h && keys[s] != kEmpty) dec(W, ctl, par, vals[s], (int64_t)h);
+    }
+  }
   {
     const int mode = kLevel == LV_WARP ? 0 : (kLevel == LV_GRID ? 3 : (hash ? 1 : 2));
     const unsigned long long w = warp_sum((unsigned long long)my_work);
@@ -899,7 +938,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
   Shared& S = *reinterpret_cast<Shared*>(smem_raw);
   uint32_t* pool = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(Shared) + 15) & ~size_t(15)));
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* wkeys = pool + warp * (2 * kWarpSlots);
+  uint32_t* wkeys = pool + warp * (3 * kWarpSlots);  // keys, values, hit counters
   uint32_t* wvals = wkeys + kWarpSlots;
   const unsigned gtid = vblock() * kPT + threadIdx.x;
   const unsigned gthreads = vgrid() * kPT;
@@ -930,6 +969,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
     }
     unsigned long long k = *(volatile unsigned long long*)&ctl->nm[par];
     if (k == kInf) {
+      unsigned long long part_target_next = 0, part_ratio_next = 0;  // range mode
       // ---- window advance (no unpeeled item left in the near list): compact the alive list
       // and take its minimum; a log2 histogram of distances to the minimum picks the window
       // bound; the near list is rebuilt from the alive list.
@@ -1002,7 +1042,17 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         __syncthreads();
         if (threadIdx.x < 66 && wh[threadIdx.x]) atomicAdd(&ctl->whist[threadIdx.x], wh[threadIdx.x]);
         if (!grid_barrier(ctl)) return false;
-        const unsigned long long target = *(volatile unsigned long long*)&ctl->part_target;
+        const unsigned long long base = *(volatile unsigned long long*)&ctl->part_target;
+        const unsigned long long done = *(volatile unsigned long long*)&ctl->part_done;
+        const unsigned long long used = *(volatile unsigned long long*)&ctl->part_used;
+        unsigned long long ratio_q = *(volatile unsigned long long*)&ctl->part_ratio_q;
+        if (used > 0 && done > 0) {
+          const unsigned long long r = min(done * 256ull / used, 256ull * 4096ull);
+          ratio_q = ratio_q ? (ratio_q + r) / 2 : r;
+        }
+        const unsigned long long target = max(1ull, ratio_q > 256 ? base * 256ull / ratio_q : base);
+        part_target_next = target;
+        part_ratio_next = ratio_q;
         unsigned long long cum = 0;
         int B = 0;
         for (; B < 65; ++B) {
@@ -1051,7 +1101,14 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
       alist_cur = na;
       if (!grid_barrier(ctl)) return false;
       phase_mark(ctl, 0);
-      if (vblock() == 0 && threadIdx.x == 0) ctl->advances += 1;
+      if (vblock() == 0 && threadIdx.x == 0) {
+        ctl->advances += 1;
+        if (range) {  // every CTA read the previous values before this barrier
+          ctl->part_used = part_target_next;
+          ctl->part_ratio_q = part_ratio_next;
+          ctl->part_done = 0;
+        }
+      }
       k = klo;
     }
     const unsigned long long win_hi = *(volatile unsigned long long*)&ctl->win_hi;
@@ -1322,6 +1379,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         ctl->n_big += nb;
         ctl->n_huge += nh;
         ctl->prev_items = ns + nb + nh;  // read by the next round's phase F after two barriers
+        if (range) ctl->part_done += *(volatile unsigned long long*)&ctl->round_est[par];
       }
     }
     if (!grid_barrier(ctl)) return false;
@@ -1747,7 +1805,7 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   }
   const Lists G0 = G;  // the full lists (version 0)
 
-  const size_t smem = ((sizeof(Shared) + 15) & ~size_t(15)) + (size_t)kBlockSlots * 2 * sizeof(uint32_t);
+  const size_t smem = ((sizeof(Shared) + 15) & ~size_t(15)) + (size_t)kBlockSlots * 3 * sizeof(uint32_t);
   auto kern = peel_kernel<kWing>;
   PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
