@@ -664,12 +664,29 @@ pb_status pb_graph_read_text(pb_ctx* ctx, const char* path, pb_graph** out) {
   });
 }
 
+static void rebind_graph(pb_graph& g) {
+  g.offV.rebind(nullptr);
+  g.edgV.rebind(nullptr);
+  g.offU.rebind(nullptr);
+  g.edgU.rebind(nullptr);
+}
+
+static void rebind_model(pb::MlpModel& m) {
+  m.params.rebind(nullptr);
+  m.grads.rebind(nullptr);
+  m.m_adam.rebind(nullptr);
+  m.v_adam.rebind(nullptr);
+  m.whalf.rebind(nullptr);
+  m.err.rebind(nullptr);
+}
+
 pb_status pb_graph_destroy(pb_graph* g) {
   if (!g) return PB_EINVAL;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(g->device);
   cudaDeviceSynchronize();
+  rebind_graph(*g);  // the context (and its stream) may already be gone
   delete g;
   cudaSetDevice(prev);
   return PB_OK;
@@ -982,6 +999,9 @@ pb_status pb_batch_destroy(pb_batch* b) {
   cudaGetDevice(&prev);
   cudaSetDevice(b->device);
   cudaDeviceSynchronize();
+  rebind_graph(b->U);
+  b->counts.rebind(nullptr);
+  b->tips.rebind(nullptr);
   delete b;
   cudaSetDevice(prev);
   return PB_OK;
@@ -1024,6 +1044,8 @@ pb_status pb_sched_model_destroy(pb_sched_model* model) {
   cudaGetDevice(&prev);
   cudaSetDevice(model->device);
   cudaDeviceSynchronize();
+  rebind_model(model->count);
+  rebind_model(model->peel);
   delete model;
   cudaSetDevice(prev);
   return PB_OK;

@@ -83,6 +83,11 @@ struct DevBuf {
   }
   T* get() const { return p; }
   size_t bytes() const { return n * sizeof(T); }
+  // The stream the buffer is freed on.  Long-lived objects (graphs, models, batches) may outlive
+  // the stream they were allocated on (a context's own stream ends with the context); their
+  // destroy functions synchronise the device and rebind their buffers to the legacy default
+  // stream, which is always valid.
+  void rebind(cudaStream_t ns) { s = ns; }
 };
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }

@@ -1139,7 +1139,9 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
           } else {
             cost = G.wk[x];
             small = cls.tip_small(G, x);
-            huge = !small && cls.tip_huge(G, x) && W.gshared != nullptr;
+            // The coarse pass's frontiers hold many heavy items at once: they run per CTA, not
+            // one after another over the whole grid.
+            huge = !small && cls.tip_huge(G, x) && W.gshared != nullptr && !range;
           }
           atomicAdd(&ctl->round_est[par], (unsigned long long)(cost > 0 ? cost : 0));
           if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
