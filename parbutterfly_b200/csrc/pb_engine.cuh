@@ -119,9 +119,8 @@ struct PeelResult {
 // Work-unit sizing of the persistent peel kernel (the defaults are the plain path's).
 struct PeelTuning {
   int64_t small_work = 512;               // items up to this work run on one warp
-  int64_t small_work_busy = 512;          // ... after a round with enough items for every warp (wing)
   int64_t huge_work = int64_t(1) << 40;   // items above this run on the whole grid
-  int64_t chunk_work = 512;               // minimum probes per CTA work unit (wing)
+  int64_t chunk_work = 512;               // probes per warp unit, minimum per CTA work unit (wing)
   int64_t units_per_cta = 4;              // CTA work units per CTA and round (wing)
   int64_t near_min = 32768;               // the near window holds at least this many items
   int64_t near_div = 64;                  // ... or alive / near_div

@@ -88,8 +88,12 @@ struct Ctl {
   // probes that walked the probe set against a binary search (the reverse direction).
   unsigned long long mode_items[4], mode_work[4], rev_work;
   unsigned prev_items;  // frontier items of the previous round
+  unsigned wunits;      // warp units of the current round (global prefix only)
 };
 constexpr unsigned kMaxGroups = 32;
+// Device memory for grid-shared dense counters (one n-sized slice per concurrent heavy tip
+// item group or per fine-pass instance with a CTA range of its own).
+constexpr int64_t kGsharedBudget = int64_t(2) << 30;
 
 
 // Live adjacency of both sides.  Lists are compacted to their live entries between launches
@@ -121,6 +125,8 @@ struct Work {
   uint32_t* fbig[2];
   uint32_t* fchunks[2];  // work units of each CTA-level item (parallel to fbig)
   uint32_t* uprefix;     // exclusive prefix of fchunks for the current round (N + 1)
+  uint32_t* fwchunks[2]; // warp units of each warp-level wing item (parallel to fsmall)
+  uint32_t* wprefix;     // exclusive prefix of fwchunks (N + 1)
   uint32_t* fhuge[2];
   uint32_t* tlist[2];
   uint32_t* gshared;   // grid-shared dense counters / probe markers for huge items (zeroed);
@@ -857,11 +863,6 @@ struct Classify {
   int64_t huge_work;   // items above this run on the whole grid
   int64_t chunk_work;  // target probes per work unit of a CTA-level wing item
   int64_t units_per_cta;  // work units per CTA a round's CTA-level wing work is cut into
-  // Wing rounds after a round of at least busy_items items (enough to keep every warp busy)
-  // send items up to small_work_busy probes to warps: many independent warp items hide the
-  // latency of their dependent loads better than CTA work units, which synchronise.
-  int64_t small_work_busy;
-  int64_t busy_items;
 
   __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const {
     return G.wk[u] <= kWarpSlots / 2 && G.wk[u] <= small_work;
@@ -1118,7 +1119,6 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
     // items is the first part of the next round's minimum.
     {
       const unsigned nl = *(volatile unsigned*)&ctl->near_len;
-      const bool busy = (int64_t)*(volatile unsigned*)&ctl->prev_items >= cls.busy_items;
       unsigned long long mn = kInf;
       for (unsigned q = gtid; q < nl; q += gthreads) {
         const uint32_t x = W.near[q];
@@ -1128,23 +1128,34 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
           W.state[x] = ACTIVE;
           bool small, huge;
           int64_t cost;
+          uint32_t wunits_of = 1;
           if (kWing) {
             const uint32_t v = G.center_of[x], u = G.u_of[x];
             const int64_t cv = cls.cost_v(G, v, u), cu = cls.cost_u(G, v, u);
             const bool fv = cv <= cu;
             cost = fv ? cv : cu;
             const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
-            small = cost <= (busy ? cls.small_work_busy : cls.small_work) && 2 * psize <= (uint32_t)kWarpSlots;
+            // Every item whose probe set fits a warp table runs on warps, cut into warp units
+            // of about chunk_work probes (first-level slices); the others on CTAs.
+            small = 2 * psize <= (uint32_t)kWarpSlots;
             huge = !small && cost > cls.huge_work && W.gshared != nullptr;
+            if (small) {
+              const int64_t d1 = fv ? G.offC[v + 1] - G.offC[v] : G.offK[u + 1] - G.offK[u];
+              int64_t units = (cost + cls.chunk_work - 1) / cls.chunk_work;
+              units = min(units, min(d1, (int64_t)4096));
+              wunits_of = (uint32_t)max(units, (int64_t)1);
+            }
           } else {
             cost = G.wk[x];
             small = cls.tip_small(G, x);
-            // The coarse pass's frontiers hold many heavy items at once: they run per CTA, not
-            // one after another over the whole grid.
-            huge = !small && cls.tip_huge(G, x) && W.gshared != nullptr && !range;
+            huge = !small && cls.tip_huge(G, x) && W.gshared != nullptr;
           }
           atomicAdd(&ctl->round_est[par], (unsigned long long)(cost > 0 ? cost : 0));
-          if (small) W.fsmall[par][atomicAdd(&ctl->flen_small[par], 1u)] = x;
+          if (small) {
+            const unsigned at = atomicAdd(&ctl->flen_small[par], 1u);
+            W.fsmall[par][at] = x;
+            if (kWing) W.fwchunks[par][at] = wunits_of;
+          }
           else if (huge) W.fhuge[par][atomicAdd(&ctl->flen_huge[par], 1u)] = x;
           else {
             const unsigned at = atomicAdd(&ctl->flen_big[par], 1u);
@@ -1178,22 +1189,78 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
     {
       if (vblock() == 0 && threadIdx.x == 0) ctl->nm[par] = kInf;  // every CTA has read it
       const unsigned ns = *(volatile unsigned*)&ctl->flen_small[par];
-      while (true) {
-        unsigned q = 0;
-        if (lane == 0) q = atomicAdd(&ctl->cur_small[par], 1u);
-        q = __shfl_sync(0xffffffffu, q, 0);
-        if (q >= ns) break;
-        const uint32_t x = W.fsmall[par][q];
-        if (W.cnt[x] == 0) continue;  // no live butterfly contains x: nothing to remove
-        if (kWing) {
-          WingEdge E;
-          E.e1 = x;
-          E.v = G.center_of[x];
-          E.u = G.u_of[x];
-          E.from_v = cls.wing_from_v(G, E.v, E.u);
-          wing_item<LV_WARP>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work);
-        } else {
+      if (!kWing) {
+        while (true) {
+          unsigned q = 0;
+          if (lane == 0) q = atomicAdd(&ctl->cur_small[par], 1u);
+          q = __shfl_sync(0xffffffffu, q, 0);
+          if (q >= ns) break;
+          const uint32_t x = W.fsmall[par][q];
+          if (W.cnt[x] == 0) continue;  // no live butterfly contains x: nothing to remove
           tip_item_warp(G, W, ctl, par, x, wkeys, wvals, work);
+        }
+      } else if (ns) {
+        // Warp units: the exclusive prefix of the warp items' unit counts (every CTA computes it
+        // in shared memory up to kLocalUnits items, else CTA 0 in global memory behind a
+        // barrier); warps claim runs of consecutive units and process an item's units of a
+        // run as one first-level slice, independently of the other warps.
+        const bool wlocal = ns <= kLocalUnits;
+        if (wlocal || vblock() == 0) {
+          uint32_t carry = 0;
+          for (uint32_t j0 = 0; j0 < ns; j0 += kPT) {
+            const uint32_t j = j0 + threadIdx.x;
+            const uint32_t c = j < ns ? W.fwchunks[par][j] : 0u;
+            uint32_t T;
+            const uint32_t incl = block_incl_scan(c, S.scan, T);
+            if (j < ns) {
+              if (wlocal) S.uprefix[j] = carry + incl - c;
+              else W.wprefix[j] = carry + incl - c;
+            }
+            carry += T;
+          }
+          if (threadIdx.x == 0) {
+            if (wlocal) S.uprefix[ns] = carry;
+            else {
+              W.wprefix[ns] = carry;
+              ctl->wunits = carry;
+            }
+          }
+        }
+        if (wlocal) __syncthreads();
+        else if (!grid_barrier(ctl)) return false;
+        const uint32_t* wpre = wlocal ? S.uprefix : W.wprefix;
+        const unsigned nwu = wlocal ? S.uprefix[ns] : *(volatile unsigned*)&ctl->wunits;
+        const unsigned Kw = max(1u, nwu / (4u * vgrid() * (kPT / 32)));
+        while (true) {
+          unsigned u = 0;
+          if (lane == 0) u = atomicAdd(&ctl->cur_small[par], Kw);
+          u = __shfl_sync(0xffffffffu, u, 0);
+          if (u >= nwu) break;
+          uint32_t lo = 0, hi = ns;  // the last item whose prefix <= u, 32-way search
+          while (hi - lo > 1) {
+            const uint32_t step = (hi - lo + 31) / 32;
+            const uint32_t idx = lo + lane * step;
+            const bool le = idx < hi && wpre[idx] <= u;
+            const unsigned bal = __ballot_sync(0xffffffffu, le);
+            lo = lo + (31 - __clz(bal)) * step;
+            hi = min(lo + step, hi);
+          }
+          const unsigned uend = min(u + Kw, nwu);
+          for (unsigned uu = u, q = lo; uu < uend; ++q) {  // uniform across the warp
+            const uint32_t base = wpre[q], next = wpre[q + 1];
+            const uint32_t c1 = min(uend, next);
+            const uint32_t x = W.fsmall[par][q];
+            if (W.cnt[x] != 0) {  // no live butterfly contains x: nothing to remove
+              WingEdge E;
+              E.e1 = x;
+              E.v = G.center_of[x];
+              E.u = G.u_of[x];
+              E.from_v = cls.wing_from_v(G, E.v, E.u);
+              wing_item<LV_WARP>(G, W, ctl, par, E, wkeys, wvals, kWarpSlots, nullptr, work, uu - base, next - base,
+                                 c1 - base);
+            }
+            uu = c1;
+          }
         }
       }
       __syncthreads();  // warp tables and the CTA table share memory
@@ -1743,10 +1810,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     if (pbase.empty()) return res;
   }
   // Grid-shared dense counters: tip peeling keeps one slice per CTA group (heavy items of a round
-  // run concurrently), up to 32 slices within 256 MB.
+  // run concurrently), up to 32 slices within kGsharedBudget.
   const int64_t gstride = std::max(G.nK, G.nC) + 1;
   const unsigned ngroups =
-      kWing ? 1u : (unsigned)std::max<int64_t>(1, std::min<int64_t>(kMaxGroups, (int64_t(256) << 20) / (4 * gstride)));
+      kWing ? 1u : (unsigned)std::max<int64_t>(1, std::min<int64_t>(kMaxGroups, kGsharedBudget / (4 * gstride)));
   DevBuf<uint32_t> gshared((size_t)gstride * ngroups, s);
   PB_CUDA_TRY(cudaMemsetAsync(gshared.get(), 0, gshared.bytes(), s));
   DevBuf<uint8_t> state(N, s), in_near(N, s);
@@ -1826,6 +1893,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
     PB_CUDA_TRY(cudaMemsetAsync(gscratch.get(), 0, gscratch.bytes(), s));
   }
   DevBuf<uint32_t> fc0(N, s), fc1(N, s), upre(N + (int64_t)pbase.size() + 1, s);
+  DevBuf<uint32_t> fw0, fw1, wpre;  // warp units of wing items
+  if (kWing) {
+    fw0.alloc(N, s);
+    fw1.alloc(N, s);
+    wpre.alloc(N + (int64_t)pbase.size() + 1, s);
+  }
   Work W{};
   W.D = (two_phase || two_phase_batch) ? snap.get() : out;
   W.cnt = cnt.get();
@@ -1842,6 +1915,9 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   W.fchunks[0] = fc0.get();
   W.fchunks[1] = fc1.get();
   W.uprefix = upre.get();
+  W.fwchunks[0] = fw0.get();
+  W.fwchunks[1] = fw1.get();
+  W.wprefix = wpre.get();
   W.fhuge[0] = fh0.get();
   W.fhuge[1] = fh1.get();
   W.gshared = gshared.get();
@@ -1878,12 +1954,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
   if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
-  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta),
-               std::max(tune.small_work, tune.small_work_busy), 2ll * grid * (kPT / 32)};
+  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
   if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);
-  if (const char* e = getenv("PB_PEEL_SMALL_WORK_BUSY")) cls.small_work_busy = std::max<int64_t>(cls.small_work, atoll(e));
   if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   DevBuf<unsigned> status(2, s);
@@ -1975,6 +2049,11 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
       x.fchunks[0] = fc0.get() + b;
       x.fchunks[1] = fc1.get() + b;
       x.uprefix = upre.get() + b + i;
+      if (kWing) {
+        x.fwchunks[0] = fw0.get() + b;
+        x.fwchunks[1] = fw1.get() + b;
+        x.wprefix = wpre.get() + b + i;
+      }
       x.fhuge[0] = fh0.get() + b;
       x.fhuge[1] = fh1.get() + b;
       x.tlist[0] = tl0.get() + b;
@@ -2098,10 +2177,18 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
       }
     }
     PB_REQUIRE(b == N, PB_ECUDA, "two-phase peel: partition sizes do not add up");
-    DevBuf<uint32_t> upre2(N + (int64_t)fws.size() + 1, s);
-    for (size_t i = 0; i < fws.size(); ++i) fws[i].uprefix = upre2.get() + fws[i].item0 + i;
+    DevBuf<uint32_t> upre2(N + (int64_t)fws.size() + 1, s), wpre2;
+    if (kWing) wpre2.alloc(N + (int64_t)fws.size() + 1, s);
+    for (size_t i = 0; i < fws.size(); ++i) {
+      fws[i].uprefix = upre2.get() + fws[i].item0 + i;
+      if (kWing) {
+        fws[i].fwchunks[0] = fw0.get() + fws[i].item0;
+        fws[i].fwchunks[1] = fw1.get() + fws[i].item0;
+        fws[i].wprefix = wpre2.get() + fws[i].item0 + i;
+      }
+    }
     const int64_t gstride_b = gstride;
-    const int64_t slices = std::max<int64_t>(1, (int64_t(256) << 20) / (4 * gstride_b));
+    const int64_t slices = std::max<int64_t>(1, kGsharedBudget / (4 * gstride_b));
     std::vector<std::unique_ptr<DevBuf<uint32_t>>> gsl;
     auto per_slot = [&](Work& x, uint32_t ncta) {
       x.gshared = nullptr;
@@ -2313,15 +2400,23 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   }
   PB_REQUIRE(b == N, PB_ECUDA, "two-phase peel: partition sizes do not add up");
   // Unit prefixes: N + 1 slots per instance (n + 1 each).
-  DevBuf<uint32_t> upre2(N + (int64_t)ws.size() + 1, s);
-  for (size_t i = 0; i < ws.size(); ++i) ws[i].uprefix = upre2.get() + ws[i].item0 + i;
+  DevBuf<uint32_t> upre2(N + (int64_t)ws.size() + 1, s), wpre2;
+  if (kWing) wpre2.alloc(N + (int64_t)ws.size() + 1, s);
+  for (size_t i = 0; i < ws.size(); ++i) {
+    ws[i].uprefix = upre2.get() + ws[i].item0 + i;
+    if (kWing) {
+      ws[i].fwchunks[0] = fw0.get() + ws[i].item0;
+      ws[i].fwchunks[1] = fw1.get() + ws[i].item0;
+      ws[i].wprefix = wpre2.get() + ws[i].item0 + i;
+    }
+  }
   const int64_t coarse_work = res.work;
   res.rounds = 0;
   res.work = 0;
   // Grid-shared counters (grid-level items) must be per instance here, since partitions share
   // item ids: instances with a CTA range of their own get one slice each while the 256 MB
   // budget lasts; the others never take the grid-level path.
-  const int64_t slices = std::max<int64_t>(1, (int64_t(256) << 20) / (4 * gstride));
+  const int64_t slices = std::max<int64_t>(1, kGsharedBudget / (4 * gstride));
   std::vector<std::unique_ptr<DevBuf<uint32_t>>> gsl;
   auto per_slot = [&](Work& x, uint32_t ncta) {
     x.gshared = nullptr;
