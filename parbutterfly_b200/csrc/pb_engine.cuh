@@ -121,6 +121,7 @@ struct PeelTuning {
   int64_t small_work = 512;               // items up to this work run on one warp
   int64_t huge_work = int64_t(1) << 40;   // items above this run on the whole grid
   int64_t chunk_work = 512;               // probes per warp unit, minimum per CTA work unit (wing)
+  bool warp_units = false;                // wing: items with warp-sized probe sets run as warp units
   int64_t units_per_cta = 4;              // CTA work units per CTA and round (wing)
   int64_t near_min = 32768;               // the near window holds at least this many items
   int64_t near_div = 64;                  // ... or alive / near_div

@@ -863,6 +863,7 @@ struct Classify {
   int64_t huge_work;   // items above this run on the whole grid
   int64_t chunk_work;  // target probes per work unit of a CTA-level wing item
   int64_t units_per_cta;  // work units per CTA a round's CTA-level wing work is cut into
+  int64_t warp_units;     // wing: every item with a warp-sized probe set runs as warp units
 
   __device__ __forceinline__ bool tip_small(const Lists& G, uint32_t u) const {
     return G.wk[u] <= kWarpSlots / 2 && G.wk[u] <= small_work;
@@ -1135,11 +1136,12 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             const bool fv = cv <= cu;
             cost = fv ? cv : cu;
             const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
-            // Every item whose probe set fits a warp table runs on warps, cut into warp units
-            // of about chunk_work probes (first-level slices); the others on CTAs.
-            small = 2 * psize <= (uint32_t)kWarpSlots;
+            // Warp-unit setting: every item whose probe set fits a warp table runs on warps, cut
+            // into warp units of about chunk_work probes (first-level slices).  Otherwise only
+            // items of at most small_work probes run on warps, whole.
+            small = 2 * psize <= (uint32_t)kWarpSlots && (cls.warp_units || cost <= cls.small_work);
             huge = !small && cost > cls.huge_work && W.gshared != nullptr;
-            if (small) {
+            if (small && cls.warp_units) {
               const int64_t d1 = fv ? G.offC[v + 1] - G.offC[v] : G.offK[u + 1] - G.offK[u];
               int64_t units = (cost + cls.chunk_work - 1) / cls.chunk_work;
               units = min(units, min(d1, (int64_t)4096));
@@ -1954,7 +1956,9 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   // wait runs out; checks that a timeout comes back as PB_ETIMEOUT with the context usable.
   if (const char* e = getenv("PB_PEEL_TEST_STUCK_BARRIER"))
     if (*e && *e != '0') hctl.test_skip_arrival = 1;
-  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta)};
+  Classify cls{tune.small_work, tune.huge_work, tune.chunk_work, std::max<int64_t>(1, tune.units_per_cta),
+               tune.warp_units ? 1 : 0};
+  if (const char* e = getenv("PB_PEEL_WARP_UNITS")) cls.warp_units = atoi(e) != 0;  // diagnostic hook
   // Thresholds may be lowered through the environment (tests use this to drive small graphs
   // through the CTA- and grid-level paths).
   if (const char* e = getenv("PB_PEEL_SMALL_WORK")) cls.small_work = atoll(e);

@@ -39,7 +39,6 @@ __global__ void count_stats_kernel(const int64_t* __restrict__ c, int64_t n, uns
 
 constexpr float kPeelMargin = 0.2016f;  // log2(1.15)
 constexpr int64_t kUnits[3] = {4, 2, 8};
-constexpr int64_t kChunk[2] = {512, 2048};
 constexpr int64_t kTipHuge[4] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) << 15, int64_t(1) << 40};
 constexpr int kCtaDiv[4] = {1, 2, 4, 8};
 // Peel-round batching: 0 runs one exact round at a time over the whole GPU; p > 0 batches the
@@ -56,10 +55,11 @@ PeelTuning peel_candidate(bool wing, int c, int resident_ctas) {
   int div = 1;
   double ppc = 0;
   if (wing) {
-    // c = (ppc * 3 + units) * 2 + chunk on the full grid; c = 0 is the plain setting.  (Fewer
-    // CTAs make the one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while small
-    // graphs suggest the opposite to a model trained on them, so the wing grid keeps every CTA.)
-    t.chunk_work = kChunk[c % 2];
+    // c = (ppc * 3 + units) * 2 + warp units on the full grid; c = 0 is the plain setting.
+    // (Fewer CTAs make the one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while
+    // small graphs suggest the opposite to a model trained on them, so the wing grid keeps every
+    // CTA.)
+    t.warp_units = (c % 2) != 0;
     t.units_per_cta = kUnits[(c / 2) % 3];
     ppc = kWingPpc[(c / 6) % 6];
   } else {
@@ -111,7 +111,7 @@ void peel_row(const float* call_f, bool wing, int c, float* row) {
   for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
   if (wing) {
     row[12] = (float)std::log2((double)t.units_per_cta);
-    row[13] = (float)std::log2((double)t.chunk_work);
+    row[13] = t.warp_units ? 1.f : 0.f;
   } else {
     row[12] = t.max_ctas > 0 ? (float)std::log2((double)((1 << 20) / t.max_ctas)) : 0.f;  // log2 of the CTA divisor
     row[13] = (float)std::log2((double)std::min<int64_t>(t.huge_work, int64_t(1) << 20));
