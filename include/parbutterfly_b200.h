@@ -302,6 +302,10 @@ pb_status pb_write_adjacency_hypergraph(const char* path, const pb_csr* g);
 /* The binary variant written by utils/hyperAdjToBinary.C: <base>.config ("nv mv nh mh") and
  * <base>.vidx / .vadj / .hidx / .hadj (32-bit offsets without the final m, 32-bit ids). */
 pb_status pb_read_binary_hypergraph(const char* base, pb_csr_owned* out);
+/* KONECT edge list (utils/KONECTtoHyperAdj.C, readKONECT utils/graphIO.h:1033-1100): leading
+ * '%' lines skipped, first column V ids, second column U ids (other columns ignored), ids of
+ * each side compacted in increasing order, lists sorted, repeated pairs dropped. */
+pb_status pb_read_konect(const char* path, pb_csr_owned* out);
 pb_status pb_write_binary_hypergraph(const char* base, const pb_csr* g);
 /* Host validation of a CSR (same checks as pb_graph_upload). */
 pb_status pb_csr_validate(const pb_csr* g, char* msg, size_t msg_len);

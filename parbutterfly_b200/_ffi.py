@@ -29,7 +29,7 @@ EXPORTS = [
     "pb_sched_train", "pb_sched_predict", "pb_sched_save", "pb_sched_load", "pb_ctx_set_sched_model",
     "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16", "pb_batch_create", "pb_batch_run",
     "pb_batch_destroy", "pb_graph_parse_text", "pb_graph_read_text", "pb_read_binary_hypergraph",
-    "pb_write_binary_hypergraph", "pb_gen_rmat_device", "pb_graph_download",
+    "pb_write_binary_hypergraph", "pb_gen_rmat_device", "pb_graph_download", "pb_read_konect",
 ]
 
 SCHED_FEATURES = 16
@@ -124,6 +124,7 @@ def lib():
         "pb_gen_batch_member": (S, [I32, C.POINTER(CSR)]),
         "pb_gen_rmat_device": (S, [P, I32, I32, I64, D, D, D, D, U64, C.POINTER(P)]),
         "pb_graph_download": (S, [P, C.POINTER(CSR)]),
+        "pb_read_konect": (S, [C.c_char_p, C.POINTER(CSR)]),
         "pb_count_total_noalloc": (S, [C.POINTER(CSR), P, P, C.c_char_p, C.c_size_t]),
         "pb_count_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
         "pb_peel_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P), C.POINTER(P)]),

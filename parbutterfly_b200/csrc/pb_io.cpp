@@ -7,6 +7,7 @@
 // whitespace separated.  The reference aborts with "Bad input file" when the header word is
 // wrong, the token count is not nv+mv+nu+mu+5, or mv != mu (:1013-1027), and exits when an
 // edge id is out of range (:1039-1051).  Here each of those is a PB_EINVAL/PB_EIO status.
+#include <algorithm>
 #include <cerrno>
 #include <cstdint>
 #include <cstdio>
@@ -230,3 +231,95 @@ pb_status pb_write_binary_hypergraph(const char* base, const pb_csr* g) {
 }
 
 }  // extern "C"
+
+// KONECT edge lists (utils/KONECTtoHyperAdj.C -> readKONECT, utils/graphIO.h:1033-1100, then
+// hypergraphFromHyperedges, :378-440): leading lines starting with '%' are skipped; the first
+// data line fixes the number of columns; every line's first column is a V id and its second a
+// U id (further columns, weights and times, are ignored); the ids of each side are compacted to
+// 0..n-1 in increasing order of the ids that occur; every adjacency list is sorted and repeated
+// pairs are dropped.
+pb_status pb_read_konect(const char* path, pb_csr_owned* out) {
+  if (!path || !out) return PB_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return PB_EIO;
+  std::vector<char> buf;
+  if (std::fseek(f, 0, SEEK_END) != 0) { std::fclose(f); return PB_EIO; }
+  long size = std::ftell(f);
+  if (size < 0) { std::fclose(f); return PB_EIO; }
+  std::rewind(f);
+  buf.resize((size_t)size);
+  if (size > 0 && std::fread(buf.data(), 1, (size_t)size, f) != (size_t)size) { std::fclose(f); return PB_EIO; }
+  std::fclose(f);
+  size_t k = 0;
+  while (k < buf.size() && buf[k] == '%') {  // comment lines at the start
+    while (k < buf.size() && buf[k] != '\n') ++k;
+    if (k < buf.size()) ++k;
+  }
+  // Columns: the words of the first data line.
+  size_t cols = 0;
+  {
+    bool prev_space = true;
+    for (size_t t = k; t < buf.size() && buf[t] != '\n'; ++t) {
+      const bool sp = buf[t] == ' ' || buf[t] == '\t' || buf[t] == '\r';
+      if (!sp && prev_space) ++cols;
+      prev_space = sp;
+    }
+  }
+  if (cols < 2) return PB_EINVAL;
+  Tokenizer t{buf.data() + k, buf.data() + buf.size()};
+  std::vector<uint64_t> vid, uid;
+  for (size_t col = 0;; col = (col + 1) % cols) {
+    const char* w;
+    size_t len;
+    if (!t.next_word(w, len)) {
+      if (col != 0) return PB_EINVAL;  // a short last line
+      break;
+    }
+    if (col >= 2) continue;  // weight / time columns
+    uint64_t x = 0;
+    for (size_t i = 0; i < len; ++i) {
+      const unsigned c = (unsigned)(w[i] - '0');
+      if (c > 9) return PB_EINVAL;
+      x = x * 10 + c;
+    }
+    (col == 0 ? vid : uid).push_back(x);
+  }
+  const size_t m = vid.size();
+  auto compact = [](std::vector<uint64_t>& ids, int64_t& n) {
+    std::vector<uint64_t> u(ids);
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    n = (int64_t)u.size();
+    for (auto& x : ids) x = (uint64_t)(std::lower_bound(u.begin(), u.end(), x) - u.begin());
+  };
+  int64_t nv = 0, nu = 0;
+  compact(vid, nv);
+  compact(uid, nu);
+  if (nv >= (int64_t(1) << 31) || nu >= (int64_t(1) << 31)) return PB_ETOOBIG;
+  std::vector<uint64_t> keys(m);
+  for (size_t e = 0; e < m; ++e) keys[e] = (vid[e] << 32) | uid[e];
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  const int64_t mm = (int64_t)keys.size();
+  if (mm > (int64_t)UINT32_MAX / 2) return PB_ETOOBIG;
+  pb_csr_owned g;
+  g.nv = nv; g.nu = nu; g.m = mm;
+  g.offsetsV = (uint32_t*)calloc((size_t)nv + 1, sizeof(uint32_t));
+  g.offsetsU = (uint32_t*)calloc((size_t)nu + 1, sizeof(uint32_t));
+  g.edgesV = (uint32_t*)malloc(sizeof(uint32_t) * (mm ? mm : 1));
+  g.edgesU = (uint32_t*)malloc(sizeof(uint32_t) * (mm ? mm : 1));
+  if (!g.offsetsV || !g.offsetsU || !g.edgesV || !g.edgesU) { pb_csr_free(&g); return PB_ENOMEM; }
+  for (int64_t e = 0; e < mm; ++e) {
+    const uint32_t v = (uint32_t)(keys[e] >> 32), u = (uint32_t)keys[e];
+    g.offsetsV[v + 1]++;
+    g.offsetsU[u + 1]++;
+    g.edgesV[e] = u;  // keys sorted by (v, u)
+  }
+  for (int64_t i = 0; i < nv; ++i) g.offsetsV[i + 1] += g.offsetsV[i];
+  for (int64_t i = 0; i < nu; ++i) g.offsetsU[i + 1] += g.offsetsU[i];
+  std::vector<uint32_t> cur(g.offsetsU, g.offsetsU + nu);
+  for (int64_t e = 0; e < mm; ++e) g.edgesU[cur[(uint32_t)keys[e]]++] = (uint32_t)(keys[e] >> 32);  // v ascending
+  *out = g;
+  return PB_OK;
+}

@@ -158,6 +158,13 @@ class BipartiteGraph:
         _ffi.check(_ffi.lib().pb_read_adjacency_hypergraph(os.fsencode(path), C.byref(s)), what=path)
         return BipartiteGraph._from_owned(s)
 
+    @staticmethod
+    def read_konect(path: str) -> "BipartiteGraph":
+        """A KONECT edge list (utils/KONECTtoHyperAdj.C semantics)."""
+        s = _ffi.CSR()
+        _ffi.check(_ffi.lib().pb_read_konect(os.fsencode(path), C.byref(s)), what=path)
+        return BipartiteGraph._from_owned(s)
+
     def write_binary(self, base: str) -> None:
         """hyperAdjToBinary's layout: base.config, .vidx, .vadj, .hidx, .hadj."""
         s = self.csr_struct()
