@@ -7,6 +7,9 @@
   plaw10m : the skewed power-law-degree workload at 1e7 edges: per-vertex counts (largest above
             2^32) and tip numbers (digests).
   c2count : the full benchmark graph (2^24 edges): per-edge counts (digest) and the total.
+  c3tip   : the skewed power-law-degree workload at full size (1e8 edges): per-vertex counts and
+            tip numbers (digests) from the oracle (64-bit buckets; the counts exceed 2^32, where
+            the reference's 32-bit buckets are not exact), pinned to the reference on plaw10m.
   c2wing  : the full benchmark graph's wing numbers (digest), from the oracle's bucket-queue
             wing peel (oracle/pb_oracle_fast.c, pinned to the reference on every smaller fixture)
             run on per-edge counts equal to the reference's; the reference's own wing peel of
@@ -118,6 +121,26 @@ def test_tip_numbers_match_reference(ctx, large, name):
         assert int(c.sum()) // 2 == int(r["use_v_wside_total"][2])
         tip = pb.peel(dg, c)
         _check(tip, r, "peel", name)
+    finally:
+        dg.close()
+
+
+@pytest.mark.gpu
+def test_power_law_workload_tip_numbers(ctx, large):
+    from parbutterfly_b200 import butterflies as pb
+    r = _rec(large, "c3tip")
+    g = BipartiteGraph.powerlaw_u(100_000, 1_000_000, 100_000_000, 2.0, 100_000, 3)
+    assert graph_digest(g) == str(r["graph_sha"])
+    dg = ctx.upload(g)
+    del g
+    try:
+        c = pb.count(dg, "BATCHS", "ADEG")
+        _check(c, r, "count", "c3tip")
+        total, rounds, w_rank = (int(x) for x in r["total_rounds_wrank"])
+        assert int(c.sum()) // 2 == total
+        tip = pb.peel(dg, c, peel_parts=1200)  # the two-phase schedule; same numbers as one round at a time
+        assert ctx.stats()["peel_rounds"] == rounds
+        _check(tip, r, "peel", "c3tip")
     finally:
         dg.close()
 
