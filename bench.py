@@ -173,7 +173,8 @@ def load_or_train_model(ctx, pb):
         return m, {"source": os.path.relpath(MODEL_PATH, ROOT), "train_s": None}
     from parbutterfly_b200 import sched_train as st
     t0 = time.perf_counter()
-    Xc, yc, Xp, yp = st.collect(ctx, st.COUNT_GRAPHS[::2], st.PEEL_GRAPHS[:2], 16, log=lambda *a: None, tip_graphs=[])
+    Xc, yc, Xp, yp = st.collect(ctx, st.COUNT_GRAPHS[::2], st.PEEL_GRAPHS[:2], 16, log=lambda *a: None, tip_graphs=[],
+                                   wing_graphs=[], batch_sets=[])
     m = st.train(ctx, Xc, yc, Xp, yp, log=lambda *a: None)
     return m, {"source": "trained at start-up (quick trace set)", "train_s": time.perf_counter() - t0}
 

@@ -148,6 +148,7 @@ struct Work {
   uint32_t my_part;
   uint32_t* part_out;
   uint32_t level;
+  const uint32_t* wgt;  // coarse pass: every item's estimated work (item_weight, capped at 2^32 - 1)
 };
 
 // Every CTA belongs to one peel instance (the whole input, or one graph of a batch, each with
@@ -1039,7 +1040,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
         for (unsigned q = gtid; q < alen2; q += gthreads) {
           const uint32_t x = W.alist[na][q];
           const unsigned long long d = (unsigned long long)W.D[x] - klo;
-          atomicAdd(&wh[d ? 64 - __clzll(d) : 0], item_weight<kWing>(G, cls, x));
+          atomicAdd(&wh[d ? 64 - __clzll(d) : 0], (unsigned long long)W.wgt[x]);
         }
         __syncthreads();
         if (threadIdx.x < 66 && wh[threadIdx.x]) atomicAdd(&ctl->whist[threadIdx.x], wh[threadIdx.x]);
@@ -1073,7 +1074,7 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
             const uint32_t x = W.alist[na][q];
             const unsigned long long d = (unsigned long long)W.D[x] - klo;
             if (d >= lo_d && d < lo_d + width)
-              atomicAdd(&wh[(unsigned)((d - lo_d) * 256ull / width)], item_weight<kWing>(G, cls, x));
+              atomicAdd(&wh[(unsigned)((d - lo_d) * 256ull / width)], (unsigned long long)W.wgt[x]);
           }
           __syncthreads();
           if (threadIdx.x < 256 && wh[threadIdx.x]) atomicAdd(&ctl->wsub[threadIdx.x], wh[threadIdx.x]);
@@ -1665,6 +1666,14 @@ __global__ void part_stats_kernel(Lists G, Classify cls, const uint32_t* __restr
   }
 }
 
+template <bool kWing>
+__global__ void item_weight_kernel(Lists G, Classify cls, int64_t N, uint32_t* wgt) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < N; x += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long w = item_weight<kWing>(G, cls, (uint32_t)x);
+    wgt[x] = (uint32_t)min(w, 0xFFFFFFFFull);
+  }
+}
+
 // gid[x] = i for the items x in [base[i], base[i + 1]) (one CTA per range).
 __global__ void range_ids_kernel(const uint32_t* __restrict__ base, uint32_t n, const uint32_t* unused, uint32_t* gid) {
   const uint32_t i = blockIdx.x;
@@ -1965,6 +1974,12 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   if (const char* e = getenv("PB_PEEL_HUGE_WORK")) cls.huge_work = atoll(e);
   if (const char* e = getenv("PB_PEEL_CHUNK_WORK")) cls.chunk_work = atoll(e);
   DevBuf<unsigned> status(2, s);
+  DevBuf<uint32_t> wgt;  // coarse passes: static per-item work estimates
+  if (two_phase || two_phase_batch) {
+    wgt.alloc(N, s);
+    PB_LAUNCH(item_weight_kernel<kWing>, grid_for(N), 256, 0, s, G0, cls, N, wgt.get());
+    W.wgt = wgt.get();
+  }
 
   // One cooperative launch of independent instances with CTA shares by weight (no compaction
   // pauses: every instance runs to its end).  per_slot may adjust each launch slot's Work.

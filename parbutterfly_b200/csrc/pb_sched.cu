@@ -55,13 +55,12 @@ PeelTuning peel_candidate(bool wing, int c, int resident_ctas) {
   int div = 1;
   double ppc = 0;
   if (wing) {
-    // c = (ppc * 3 + units) * 2 + warp units on the full grid; c = 0 is the plain setting.
-    // (Fewer CTAs make the one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while
-    // small graphs suggest the opposite to a model trained on them, so the wing grid keeps every
-    // CTA.)
-    t.warp_units = (c % 2) != 0;
-    t.units_per_cta = kUnits[(c / 2) % 3];
-    ppc = kWingPpc[(c / 6) % 6];
+    // c = ppc * 3 + units on the full grid; c = 0 is the plain setting.  (Fewer CTAs make the
+    // one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while small graphs suggest
+    // the opposite to a model trained on them, so the wing grid keeps every CTA; warp units are
+    // slower on it too and stay out of the grid.)
+    t.units_per_cta = kUnits[c % 3];
+    ppc = kWingPpc[(c / 3) % 6];
   } else {
     // c = (ppc * 4 + huge) * 4 + cta divisor; c = 0 is the plain setting.
     div = kCtaDiv[c % 4];
@@ -111,7 +110,7 @@ void peel_row(const float* call_f, bool wing, int c, float* row) {
   for (int k = 0; k < kPeelCallFeatures; ++k) row[k] = call_f[k];
   if (wing) {
     row[12] = (float)std::log2((double)t.units_per_cta);
-    row[13] = t.warp_units ? 1.f : 0.f;
+    row[13] = 0.f;
   } else {
     row[12] = t.max_ctas > 0 ? (float)std::log2((double)((1 << 20) / t.max_ctas)) : 0.f;  // log2 of the CTA divisor
     row[13] = (float)std::log2((double)std::min<int64_t>(t.huge_work, int64_t(1) << 20));

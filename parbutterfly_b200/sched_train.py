@@ -7,8 +7,8 @@ uniform graphs.  With tracing in explore mode the plain path logs
     with a random valid aggregation mode per item (target log2 SM cycles of the item);
   - peel:  one row per tip / wing peel call, sweeping the setting grid (round batching of the
     two-phase schedule, work units, grid-level thresholds, CTA count; target log2 ms of the
-    call); larger graphs are traced for tip peeling only, and for wing peeling over the
-    round-batching settings only.
+    call); larger graphs are traced for tip peeling only or wing peeling only, and batches of
+    128 / 256 graphs (batch-generator members 1000+) for batch tip peeling.
 Both MLPs are then trained on the GPU (tensor-core forward / backward, Adam) and saved.
 
     python -m parbutterfly_b200.sched_train --out sched.bin [--quick]
@@ -56,7 +56,10 @@ def make(kind, args, seed) -> BipartiteGraph:
     return BipartiteGraph.uniform(*args, seed)
 
 
-# Larger graphs traced for wing peeling with the plain work units and every round batching.
+# Batches of graphs traced for tip peeling over every setting: members 1000+ of the batch
+# generator (seeds 5000+; the benchmark batch uses members 0-255).
+BATCH_SETS = [list(range(1000, 1128)), list(range(1200, 1456))]
+# Larger graphs traced for wing peeling over every setting.
 WING_GRAPHS = [
     ("rmat", (18, 16, 1 << 22, 0.55, 0.15, 0.15, 0.15), 7301),
     ("rmat", (19, 17, 1 << 23, 0.45, 0.25, 0.15, 0.15), 7302),
@@ -64,7 +67,7 @@ WING_GRAPHS = [
 
 
 def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS, peel_settings=48, log=print,
-            tip_graphs=TIP_GRAPHS, wing_graphs=WING_GRAPHS):
+            tip_graphs=TIP_GRAPHS, wing_graphs=WING_GRAPHS, batch_sets=BATCH_SETS):
     """Explore-mode traces: returns (Xc, yc, Xp, yp)."""
     pb.trace_clear(ctx)
     pb.trace_set(ctx, "explore", seed=1)
@@ -99,11 +102,21 @@ def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS,
             t0 = time.perf_counter()
             dg = ctx.upload(make(*spec))
             ce = pb.count_e(dg, "BATCHS", "ADEG")
-            for b in range(6):  # every round batching with the plain work units: candidates 0, 6, ..., 30
-                pb.trace_set(ctx, "explore", seed=6 * b)  # the sweep position of the next peel call
+            for c in range(18):  # every wing candidate (the sweep position of the next peel call)
+                pb.trace_set(ctx, "explore", seed=c)
                 pb.peel_e(dg, ce)
             dg.close()
             log(f"[sched_train] wing traces {spec[0]}{spec[1][:3]}: {time.perf_counter() - t0:.1f} s")
+        for members in batch_sets:
+            t0 = time.perf_counter()
+            dgs = [ctx.upload(BipartiteGraph.batch_member(k)) for k in members]
+            cs = pb.count_batch(dgs, "BATCHS", "ADEG")
+            for c in range(48):  # every tip candidate
+                pb.trace_set(ctx, "explore", seed=c)
+                pb.peel_batch(dgs, cs)
+            for dg in dgs:
+                dg.close()
+            log(f"[sched_train] batch tip traces {len(members)} graphs: {time.perf_counter() - t0:.1f} s")
     finally:
         pb.trace_set(ctx, "off")
     Xc, yc = pb.trace_rows(ctx, pb.SchedModel.COUNT)
@@ -129,10 +142,10 @@ def main():
     ap.add_argument("--quick", action="store_true", help="fewer graphs and peel settings")
     a = ap.parse_args()
     ctx = pb.Context(a.device)
-    cg, pg, ps, tg, wg = COUNT_GRAPHS, PEEL_GRAPHS, 48, TIP_GRAPHS, WING_GRAPHS
+    cg, pg, ps, tg, wg, bs = COUNT_GRAPHS, PEEL_GRAPHS, 48, TIP_GRAPHS, WING_GRAPHS, BATCH_SETS
     if a.quick:
-        cg, pg, ps, tg, wg = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16, [], []
-    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps, tip_graphs=tg, wing_graphs=wg)
+        cg, pg, ps, tg, wg, bs = COUNT_GRAPHS[::2], PEEL_GRAPHS[:2], 16, [], [], []
+    Xc, yc, Xp, yp = collect(ctx, cg, pg, ps, tip_graphs=tg, wing_graphs=wg, batch_sets=bs)
     m = train(ctx, Xc, yc, Xp, yp)
     m.save(a.out)
     print(f"[sched_train] saved {a.out}")
