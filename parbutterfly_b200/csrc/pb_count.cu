@@ -318,9 +318,19 @@ __device__ __forceinline__ void block_wedges(uint32_t b, uint32_t e, const Param
       const uint32_t k0 = (p - first_piece) * kPiece;
       const uint32_t kend = min(k0 + kPiece, S.len[lo]);
       const uint32_t vsj = S.vs[lo], vtj = S.vt[lo];
-      for (uint32_t k = k0 + lane; k < kend; k += 32) {
-        const uint32_t slot2 = vsj + k;
-        if (slot_ok(P, slot2, 21)) f(j0 + lo, vtj, slot2, P.adj[slot2]);
+      // Vectorised walk: lane t takes the aligned group of four entries at g + 4t (one 16-byte
+      // load; the adjacency array is 16-byte aligned and padded to whole groups), and uses the
+      // entries inside the piece [vsj + k0, vsj + kend).
+      const uint32_t pbeg = vsj + k0, pend = vsj + kend;
+      for (uint32_t g = (pbeg & ~3u) + 4u * lane; g < pend; g += 128u) {
+        if (!slot_ok(P, g, 21)) break;
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(P.adj + g));
+        const uint32_t x[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (uint32_t r = 0; r < 4; ++r) {
+          const uint32_t slot2 = g + r;
+          if (slot2 >= pbeg && slot2 < pend && slot_ok(P, slot2, 21)) f(j0 + lo, vtj, slot2, x[r]);
+        }
       }
     }
     __syncthreads();

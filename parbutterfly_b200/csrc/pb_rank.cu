@@ -329,7 +329,9 @@ void build_ranked_csr(const pb_graph& g, Ranked& R, bool with_eout, cudaStream_t
   const int64_t n = R.n;
   R.m2 = 2 * g.m;
   R.off.alloc(n + 1, s);
-  R.adj.alloc(R.m2 > 0 ? R.m2 : 1, s);
+  // Padded to whole 16-byte groups: the aggregators walk rows with 16-byte loads of aligned
+  // groups of four entries (entries outside the row are masked, never used).
+  R.adj.alloc((size_t)((R.m2 + 3) & ~int64_t(3)) + 4, s);
   if (with_eout) R.eout.alloc(R.m2 > 0 ? R.m2 : 1, s);
   R.max_deg = g.max_deg;
   if (n == 0) {
