@@ -1464,9 +1464,14 @@ __device__ bool peel_instance(const Lists& G, const Work& W, Ctl* ctl, const Cla
   return true;
 }
 
-template <bool kWing>
-__global__ void __launch_bounds__(kPT) peel_kernel(Lists G, const Lists* levels, Instances I, Ctl* ctls,
-                                                   Classify cls) {
+// kMinBlocks: CTAs per SM the register allocation must allow.  2 caps a thread at 64 registers
+// (some spill); 1 leaves about 108 and no spills, at half the resident warps.  The single-
+// instance tip peel runs faster on the latter (fewer CTAs also shorten its grid barriers: R-MAT
+// 2^24, one round at a time, 2.36 s -> 1.60 s); wing peeling and batches keep two CTAs per SM
+// (the wing peel's intersections need the warps: 18.5 s against 19.6 s).
+template <bool kWing, int kMinBlocks>
+__global__ void __launch_bounds__(kPT, kMinBlocks) peel_kernel(Lists G, const Lists* levels, Instances I, Ctl* ctls,
+                                                               Classify cls) {
   // levels: the live-list versions of a two-phase fine pass (an instance reads
   // levels[W.level]); null: every instance reads G.
   __shared__ Work sW;
@@ -1886,7 +1891,10 @@ PeelResult run_peel(const pb_graph& g, int use_v, const int64_t* counts, int64_t
   const Lists G0 = G;  // the full lists (version 0)
 
   const size_t smem = ((sizeof(Shared) + 15) & ~size_t(15)) + (size_t)kBlockSlots * 3 * sizeof(uint32_t);
-  auto kern = peel_kernel<kWing>;
+  void (*kern)(Lists, const Lists*, Instances, Ctl*, Classify) = peel_kernel<kWing, 2>;
+  if constexpr (!kWing) {
+    if (!batch) kern = peel_kernel<false, 1>;
+  }
   PB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   PB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
