@@ -573,6 +573,74 @@ def c4_arm(args, rank, world, local):
         print(json.dumps(line))
 
 
+C5 = {
+    "workload": "bipartite R-MAT 2^26 x 2^24, m=1e9, (a,b,c,d)=(.57,.19,.19,.05), seed 5, generated on the device; "
+                "ADEG rank, per-VERT BATCHS count + tip peel",
+    "nv": 1 << 26, "nu": 1 << 24, "m": 1_000_000_000, "rank_type": "ADEG", "count_type": "BATCHS", "per": "VERT",
+    "peel_type": "BATCHS", "l2": "inputs far larger than L2",
+}
+
+
+def c5_arm(args, rank, world, local):
+    """The 1e9-edge R-MAT: per-vertex count + tip peel with the plain fixed strategy and with the
+    learned scheduler, one timed step each after an untimed count (a step takes minutes; the
+    graph is generated on the device, the host generator would need tens of GB).  Both steps
+    must give identical counts and tip numbers."""
+    import numpy as np
+    import torch
+    from parbutterfly_b200 import butterflies as pb
+
+    stream = torch.cuda.Stream(local)
+    torch.cuda.set_stream(stream)
+    ctx = pb.Context(local, stream=stream.cuda_stream)
+    model, model_info = load_or_train_model(ctx, pb)
+    model.attach()
+    t0 = time.perf_counter()
+    dg = pb.gen_rmat_device(ctx, 26, 24, C5["m"], 0.57, 0.19, 0.19, 0.05, 5)
+    gen_s = time.perf_counter() - t0
+    counts = torch.zeros(dg.nu if pb.cmp_wedge_counts(dg)[0] else dg.nv, dtype=torch.int64, device="cuda")
+    tips = torch.zeros_like(counts)
+    pb.count(dg, C5["count_type"], C5["rank_type"], out=counts)  # untimed
+    res = {}
+    ref = None
+    for sched in ("plain", "learned"):
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        pb.count(dg, C5["count_type"], C5["rank_type"], out=counts, sched=sched)
+        e1.record(stream)
+        s1 = ctx.stats()
+        pb.peel(dg, counts, C5["peel_type"], out=tips, sched=sched)
+        e2.record(stream)
+        e2.synchronize()
+        s2 = ctx.stats()
+        c_ms, p_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+        out = (counts.cpu().numpy(), tips.cpu().numpy())
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out[0], ref[0]) and np.array_equal(out[1], ref[1]), "learned and plain results differ"
+        res[sched] = {"ms_per_step": c_ms + p_ms, "count_ms": c_ms, "peel_ms": p_ms,
+                      "value": s1["w_rank"] / ((c_ms + p_ms) / 1e3), "peel_rounds": s2["peel_rounds"],
+                      "peel_parts": s2["peel_parts"], "peel_choice": s2["sched_choice"]}
+    w_rank = int(s1["w_rank"])
+    line = {
+        "metric": "wedges/s", "value": res["learned"]["value"], "unit": "wedges/s", "n_gpus": world, "steps": 1,
+        "warmup": 0, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded R-MAT generated on the device)",
+        "config": dict(C5, w_rank=w_rank, gen_s=gen_s, total=int(ref[0].sum()) // 2,
+                       note="one timed step per arm after an untimed count"),
+        "plain": res["plain"], "learned": res["learned"],
+        "learned_over_plain": res["plain"]["ms_per_step"] / res["learned"]["ms_per_step"],
+        "sched_model": model_info,
+    }
+    dg.close()
+    model.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -581,8 +649,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 256-graph batch object of the default line")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
-                    help="c2: the R-MAT 2^24 count + wing peel (default); c4: the 256-graph batch")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"],
+                    help="c2: the R-MAT 2^24 count + wing peel (default); c4: the 256-graph batch; "
+                         "c5: the 1e9-edge R-MAT count + tip peel (minutes per step)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     try:
@@ -590,6 +659,8 @@ def main():
             reference_arm(args, rank, world)
         elif args.workload == "c4":
             c4_arm(args, rank, world, local)
+        elif args.workload == "c5":
+            c5_arm(args, rank, world, local)
         else:
             our_arm(args, rank, world, local)
     finally:

@@ -4,6 +4,7 @@
 // call-level features.  Candidates are a fixed grid of
 // PeelTuning values per peel kind; candidate 0 is the plain path's setting.  The counting side
 // (per-item aggregation modes) lives with the aggregator in pb_count.cu.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -121,13 +122,20 @@ void peel_row(const float* call_f, bool wing, int c, float* row) {
 
 int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {
   const int nc = peel_candidates(wing);
-  // Calls unlike the training data (a call feature more than 4 standard deviations from the
-  // training mean) keep the plain setting: the model has no basis to predict them.
-  bool in_range = true;
-  for (int k = 0; k < kPeelCallFeatures; ++k)
-    if (model.x_scale[k] > 0.f && std::fabs((call_f[k] - model.x_mean[k]) * model.x_scale[k]) > 4.f) in_range = false;
+  // A call unlike the training data (a call feature more than 4 standard deviations from the
+  // training mean, e.g. a graph far larger than any traced one) is evaluated at the nearest
+  // point of that range: its features are clamped to mean +- 4 deviations, so the model ranks
+  // the settings as for the most similar traced calls.  The margin below still applies.
+  float cf[kPeelCallFeatures];
+  for (int k = 0; k < kPeelCallFeatures; ++k) {
+    cf[k] = call_f[k];
+    if (model.x_scale[k] > 0.f) {
+      const float lim = 4.f / model.x_scale[k];
+      cf[k] = std::min(std::max(cf[k], model.x_mean[k] - lim), model.x_mean[k] + lim);
+    }
+  }
   std::vector<float> X((size_t)nc * kMlpIn), y(nc);
-  for (int c = 0; c < nc; ++c) peel_row(call_f, wing, c, X.data() + (size_t)c * kMlpIn);
+  for (int c = 0; c < nc; ++c) peel_row(cf, wing, c, X.data() + (size_t)c * kMlpIn);
   DevBuf<float> Xd(X.size(), s), yd(nc, s);
   PB_CUDA_TRY(cudaMemcpyAsync(Xd.get(), X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s));
   model.predict_dev(Xd.get(), nc, yd.get(), s);
@@ -137,7 +145,7 @@ int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log
   for (int c = 1; c < nc; ++c)
     if (y[c] < y[best]) best = c;
   // Another setting replaces the plain one only when predicted at least 15% faster.
-  if (!in_range || y[0] - y[best] < kPeelMargin) best = 0;
+  if (y[0] - y[best] < kPeelMargin) best = 0;
   if (pred_log2ms) *pred_log2ms = y[best];
   return best;
 }
