@@ -44,7 +44,6 @@ constexpr int64_t kTipHuge[4] = {int64_t(1) << 13, int64_t(1) << 11, int64_t(1) 
 constexpr int kCtaDiv[4] = {1, 2, 4, 8};
 // Peel-round batching: 0 runs one exact round at a time over the whole GPU; p > 0 batches the
 // rounds into about p partitions per CTA (the two-phase schedule).
-constexpr double kWingPpc[6] = {0, 0.5, 1, 2, 4, 8};
 constexpr double kTipPpc[3] = {0, 1, 4};
 
 }  // namespace
@@ -56,12 +55,12 @@ PeelTuning peel_candidate(bool wing, int c, int resident_ctas) {
   int div = 1;
   double ppc = 0;
   if (wing) {
-    // c = ppc * 3 + units on the full grid; c = 0 is the plain setting.  (Fewer CTAs make the
-    // one-instance wing peel of a 2^24-edge graph 1.2-1.8x slower, while small graphs suggest
-    // the opposite to a model trained on them, so the wing grid keeps every CTA; warp units are
-    // slower on it too and stay out of the grid.)
+    // c = units on the full grid; c = 0 is the plain setting.  Wing peels run one round at a
+    // time: the two-phase schedule enumerates every butterfly twice, which made the 2^24-edge
+    // wing peel 1.2-1.6x slower at every partition count measured, and a model trained on
+    // smaller graphs (where it pays) picked it there.  Fewer CTAs are slower there too (1.2-1.8x),
+    // and warp units are no faster, so both stay out of the grid.
     t.units_per_cta = kUnits[c % 3];
-    ppc = kWingPpc[(c / 3) % 6];
   } else {
     // c = (ppc * 4 + huge) * 4 + cta divisor; c = 0 is the plain setting.
     div = kCtaDiv[c % 4];
@@ -122,20 +121,15 @@ void peel_row(const float* call_f, bool wing, int c, float* row) {
 
 int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log2ms, cudaStream_t s) {
   const int nc = peel_candidates(wing);
-  // A call unlike the training data (a call feature more than 4 standard deviations from the
-  // training mean, e.g. a graph far larger than any traced one) is evaluated at the nearest
-  // point of that range: its features are clamped to mean +- 4 deviations, so the model ranks
-  // the settings as for the most similar traced calls.  The margin below still applies.
-  float cf[kPeelCallFeatures];
-  for (int k = 0; k < kPeelCallFeatures; ++k) {
-    cf[k] = call_f[k];
-    if (model.x_scale[k] > 0.f) {
-      const float lim = 4.f / model.x_scale[k];
-      cf[k] = std::min(std::max(cf[k], model.x_mean[k] - lim), model.x_mean[k] + lim);
-    }
-  }
+  // Calls unlike the training data (a call feature more than 4 standard deviations from the
+  // training mean) keep the plain setting: the model has no basis to predict them.  (Evaluating
+  // them at the edge of the training range instead chose round batchings that ran 1.6x slower
+  // on the 2^24-edge wing peel and 2.2x slower on the 1e9-edge tip peel.)
+  bool in_range = true;
+  for (int k = 0; k < kPeelCallFeatures; ++k)
+    if (model.x_scale[k] > 0.f && std::fabs((call_f[k] - model.x_mean[k]) * model.x_scale[k]) > 4.f) in_range = false;
   std::vector<float> X((size_t)nc * kMlpIn), y(nc);
-  for (int c = 0; c < nc; ++c) peel_row(cf, wing, c, X.data() + (size_t)c * kMlpIn);
+  for (int c = 0; c < nc; ++c) peel_row(call_f, wing, c, X.data() + (size_t)c * kMlpIn);
   DevBuf<float> Xd(X.size(), s), yd(nc, s);
   PB_CUDA_TRY(cudaMemcpyAsync(Xd.get(), X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, s));
   model.predict_dev(Xd.get(), nc, yd.get(), s);
@@ -145,7 +139,7 @@ int choose_peel(MlpModel& model, const float* call_f, bool wing, float* pred_log
   for (int c = 1; c < nc; ++c)
     if (y[c] < y[best]) best = c;
   // Another setting replaces the plain one only when predicted at least 15% faster.
-  if (y[0] - y[best] < kPeelMargin) best = 0;
+  if (!in_range || y[0] - y[best] < kPeelMargin) best = 0;
   if (pred_log2ms) *pred_log2ms = y[best];
   return best;
 }

@@ -7,7 +7,7 @@
 namespace pb {
 
 constexpr int kPeelCallFeatures = 12;  // call-level features; 4 candidate slots follow
-constexpr int kWingCandidates = 18;    // 6 round batchings x 3 work-unit counts (full grid)
+constexpr int kWingCandidates = 3;     // 3 work-unit counts (full grid, one round at a time)
 constexpr int kTipCandidates = 48;     // 3 round batchings x 4 grid-level thresholds x 4 CTA counts
 
 int peel_candidates(bool wing);

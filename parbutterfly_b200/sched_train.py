@@ -5,8 +5,8 @@ workloads (other seeds and sizes): bipartite R-MAT with three skews, Zipf-endpoi
 uniform graphs.  With tracing in explore mode the plain path logs
   - count: one row per block-aggregator item of every count call (VERT and EDGE, HASH),
     with a random valid aggregation mode per item (target log2 SM cycles of the item);
-  - peel:  one row per tip / wing peel call, sweeping the setting grid (round batching of the
-    two-phase schedule, work units, grid-level thresholds, CTA count; target log2 ms of the
+  - peel:  one row per tip / wing peel call, sweeping the setting grid (tip: round batching of
+    the two-phase schedule, grid-level thresholds, CTA count; wing: work units; target log2 ms of the
     call); larger graphs are traced for tip peeling only or wing peeling only, and batches of
     128 / 256 graphs (batch-generator members 1000+) for batch tip peeling.
 Both MLPs are then trained on the GPU (tensor-core forward / backward, Adam) and saved.
@@ -102,7 +102,7 @@ def collect(ctx: pb.Context, count_graphs=COUNT_GRAPHS, peel_graphs=PEEL_GRAPHS,
             t0 = time.perf_counter()
             dg = ctx.upload(make(*spec))
             ce = pb.count_e(dg, "BATCHS", "ADEG")
-            for c in range(18):  # every wing candidate (the sweep position of the next peel call)
+            for c in range(3):  # every wing candidate (the sweep position of the next peel call)
                 pb.trace_set(ctx, "explore", seed=c)
                 pb.peel_e(dg, ce)
             dg.close()

@@ -169,7 +169,7 @@ def test_peel_explore_every_setting_exact_and_learned(ctx):
         np.testing.assert_array_equal(pb.peel_e(dg, ce, sched="learned"), pb.peel_e(dg, ce))
         pb.peel_e(dg, ce, sched="learned")
         st = ctx.stats()
-        assert st["sched_used"] == 1 and 0 <= st["sched_choice"] < 18 and st["sched_pred"] > 0
+        assert st["sched_used"] == 1 and 0 <= st["sched_choice"] < 3 and st["sched_pred"] > 0
         pb.peel(dg, c, sched="learned")
         assert 0 <= ctx.stats()["sched_choice"] < 48
     finally:
