@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libpboracle.so")
 HARNESS_OMP = os.path.join(HERE, "_ref", "ref_harness_omp")
 HARNESS_SER = os.path.join(HERE, "_ref", "ref_harness_ser")
+HARNESS_FWD = os.path.join(HERE, "_ref", "ref_harness_fwd")  # built without INVERSE
 
 RANK = {"SIDE": 0, "COCORE": 1, "ACOCORE": 2, "DEG": 3, "ADEG": 4}
 PER = {"VERT": 0, "EDGE": 1, "TOTAL": 2}
@@ -155,9 +156,10 @@ def have_reference(serial: bool = False) -> bool:
 
 
 def run_reference(g, per="VERT", count_type="BATCHS", rank="ADEG", peel="NONE", rounds=1, threads=None,
-                  serial=False, timeout=None):
-    """Runs the compiled reference on g.  Returns dict(use_v, w_side, total, count, peel, count_s, peel_s)."""
-    exe = HARNESS_SER if serial else HARNESS_OMP
+                  serial=False, timeout=None, forward=False):
+    """Runs the compiled reference on g.  Returns dict(use_v, w_side, total, count, peel, count_s, peel_s).
+    forward: the build without INVERSE (the reference's other wedge direction)."""
+    exe = HARNESS_FWD if forward else (HARNESS_SER if serial else HARNESS_OMP)
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     env = dict(os.environ)

@@ -28,7 +28,11 @@
 
 #define HYPER 1
 #define MCX16 1
+// BipartiteButterflies.C:10 defines INVERSE (the direction its driver ships with); the
+// PB_REF_FORWARD build leaves it undefined to run the reference's other wedge direction.
+#ifndef PB_REF_FORWARD
 #define INVERSE 1
+#endif
 
 #include "hypergraphIO.h"
 #include "index_map.h"
