@@ -47,6 +47,8 @@ typedef enum { PB_SORT = 0, PB_ASORT, PB_HASH, PB_AHASH, PB_HIST, PB_AHIST, PB_B
 typedef enum { PB_SIDE = 0, PB_COCORE, PB_ACOCORE, PB_DEG, PB_ADEG } pb_rank_type;
 typedef enum { PB_PSORT = 0, PB_PHASH, PB_PHIST, PB_PBATCHS, PB_PBATCHWA } pb_peel_type;
 typedef enum { PB_VERT = 0, PB_EDGE, PB_TOTAL } pb_per_type;
+/* SparseType, butterfly_utils.h:28 (same values). */
+typedef enum { PB_NOSPARSE = 0, PB_SPARSE_COLOR, PB_SPARSE_EDGE } pb_sparse_type;
 
 /* Strategy scheduler: PLAIN = the fixed strategy named by count_type; LEARNED = per-block
  * strategy picked by the learned scheduler (results are identical either way). */
@@ -306,6 +308,19 @@ pb_status pb_read_binary_hypergraph(const char* base, pb_csr_owned* out);
  * '%' lines skipped, first column V ids, second column U ids (other columns ignored), ids of
  * each side compacted in increasing order, lists sorted, repeated pairs dropped. */
 pb_status pb_read_konect(const char* path, pb_csr_owned* out);
+/* Sparsification for approximate total counts (-sparseType / -s, -d of BipartiteButterflies.C:
+ * 175-193, 333-340), host preprocessing before the GPU count.  PB_SPARSE_EDGE keeps each edge
+ * whose hash of (v, u, seed) is 0 mod denom (eSparseBipartite, butterfly_utils.h:790-890);
+ * PB_SPARSE_COLOR colours every vertex by a hash of (id, seed) mod denom and keeps the edges
+ * whose endpoints share a colour (clrSparseBipartite, :900-996).  Both then drop the vertices
+ * left without edges and renumber each side in increasing order (delZeroDeg, :744-786).  The
+ * reference's driver uses seed 0.  Release the result with pb_csr_free. */
+pb_status pb_sparsify_bipartite(const pb_csr* g, int32_t sparse_type, int64_t denom, int64_t seed,
+                                pb_csr_owned* out);
+/* The estimate printed for a sparsified graph's total count (BipartiteButterflies.C:213-214):
+ * count * denom^3 (colour) or count * denom^4 (edge), computed in double precision and
+ * truncated to an integer, as the reference does. */
+int64_t pb_sparse_estimate(int64_t sparse_count, int32_t sparse_type, int64_t denom);
 pb_status pb_write_binary_hypergraph(const char* base, const pb_csr* g);
 /* Host validation of a CSR (same checks as pb_graph_upload). */
 pb_status pb_csr_validate(const pb_csr* g, char* msg, size_t msg_len);

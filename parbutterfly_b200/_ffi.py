@@ -30,13 +30,15 @@ EXPORTS = [
     "pb_trace_set", "pb_trace_rows", "pb_trace_clear", "pb_tc_gemm_bf16", "pb_batch_create", "pb_batch_run",
     "pb_batch_destroy", "pb_graph_parse_text", "pb_graph_read_text", "pb_read_binary_hypergraph",
     "pb_write_binary_hypergraph", "pb_gen_rmat_device", "pb_graph_download", "pb_read_konect",
+    "pb_sparsify_bipartite", "pb_sparse_estimate",
 ]
 
 SCHED_FEATURES = 16
-SCHED_WING_CANDIDATES = 6
-SCHED_TIP_CANDIDATES = 32
+SCHED_WING_CANDIDATES = 3
+SCHED_TIP_CANDIDATES = 48
 SCHED_COUNT, SCHED_PEEL = 0, 1
 TRACE_OFF, TRACE_PLAIN, TRACE_EXPLORE = 0, 1, 2
+SPARSE = {"NONE": 0, "COLOR": 1, "EDGE": 2}  # SparseType, butterfly_utils.h:28
 
 
 class PBLibraryMissing(RuntimeError):
@@ -125,6 +127,8 @@ def lib():
         "pb_gen_rmat_device": (S, [P, I32, I32, I64, D, D, D, D, U64, C.POINTER(P)]),
         "pb_graph_download": (S, [P, C.POINTER(CSR)]),
         "pb_read_konect": (S, [C.c_char_p, C.POINTER(CSR)]),
+        "pb_sparsify_bipartite": (S, [C.POINTER(CSR), I32, I64, I64, C.POINTER(CSR)]),
+        "pb_sparse_estimate": (I64, [I64, I32, I64]),
         "pb_count_total_noalloc": (S, [C.POINTER(CSR), P, P, C.c_char_p, C.c_size_t]),
         "pb_count_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P)]),
         "pb_peel_vert_batch": (S, [P, C.POINTER(P), I32, C.POINTER(Opts), C.POINTER(P), C.POINTER(P)]),

@@ -6,8 +6,8 @@
 //   -sparseType/-s, -r; Compute() at :75-277 and parallel_main() at :283-355.  Timer lines use
 //   the reference's "<name> : <seconds>" format (ligra/gettime.h:87-96, setprecision(3)).
 // Additions: -sched {plain,learned}, -schedModel <file>, -autotune, -device N.
-// Differences: sparsification (-sparseType EDGE/COLOR) is approximate counting, outside this
-// path; it is rejected with an error instead of being run.
+// Sparsification (-sparseType EDGE/COLOR, -s, -d) sparsifies each round's graph on the host
+// (pb_sparsify_bipartite, seed 0 as the reference's driver) and prints the scaled estimate.
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -167,12 +167,14 @@ int main(int argc, char** argv) {
   }
   o.max_wedges = P.lng("-m", 2577500000L);
   o.max_array_size = P.lng("-a", 23090996160L);
-  long sparse = P.lng("-s", LONG_MAX);
-  std::string ss = P.str("-sparseType", "");
-  if ((sparse != LONG_MAX && sparse != 0) || ss == "EDGE" || ss == "COLOR") {
-    std::cerr << "sparsification (approximate counting) is not part of this build" << std::endl;
-    return 1;
-  }
+  // Sparsification (:175-193): -d denom, -s 0/1/2 or -sparseType COLOR/EDGE; forces TOTAL.
+  const long denom = P.lng("-d", 25);
+  const long sparse_num = P.lng("-s", LONG_MAX);
+  const std::string ss = P.str("-sparseType", "");
+  int32_t sparse = PB_NOSPARSE;
+  if (sparse_num == LONG_MAX) sparse = ss == "EDGE" ? PB_SPARSE_EDGE : (ss == "COLOR" ? PB_SPARSE_COLOR : PB_NOSPARSE);
+  else sparse = sparse_num == 1 ? PB_SPARSE_COLOR : (sparse_num == 2 ? PB_SPARSE_EDGE : PB_NOSPARSE);
+  if (sparse != PB_NOSPARSE) o.per_type = PB_TOTAL;
   if (o.per_type == PB_TOTAL) nopeel = true;
   o.sched = P.str("-sched", "plain") == "learned" ? PB_SCHED_LEARNED : PB_SCHED_PLAIN;
   for (int i = 1; i < argc - 1; ++i)
@@ -210,6 +212,14 @@ int main(int argc, char** argv) {
       pb_ctx_destroy(ctx);
       return 1;
     }
+    if (sparse != PB_NOSPARSE) {  // the reference sparsifies each round's graph with seed 0 (:333-340)
+      pb_csr full{h.nv, h.nu, h.m, h.offsetsV, h.edgesV, h.offsetsU, h.edgesU};
+      pb_csr_owned hs;
+      st = pb_sparsify_bipartite(&full, sparse, denom, 0, &hs);
+      pb_csr_free(&h);
+      if (st != PB_OK) return fail(ctx, st, "pb_sparsify_bipartite");
+      h = hs;
+    }
     pb_csr c{h.nv, h.nu, h.m, h.offsetsV, h.edgesV, h.offsetsU, h.edgesU};
     pb_graph* g = nullptr;
     double t0 = now();
@@ -227,6 +237,7 @@ int main(int argc, char** argv) {
       st = pb_count_total(ctx, g, &o, &nb);
       if (st != PB_OK) return fail(ctx, st, "pb_count_total");
       report(count_name(o.count_type), now() - t1);
+      if (sparse != PB_NOSPARSE) nb = pb_sparse_estimate(nb, sparse, denom);
       std::cout << "number of butterflies: " << nb << "\n";
     } else if (o.per_type == PB_VERT) {
       const int64_t nc = use_v ? h.nu : h.nv;

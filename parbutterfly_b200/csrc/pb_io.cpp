@@ -9,6 +9,7 @@
 // edge id is out of range (:1039-1051).  Here each of those is a PB_EINVAL/PB_EIO status.
 #include <algorithm>
 #include <cerrno>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -322,4 +323,109 @@ pb_status pb_read_konect(const char* path, pb_csr_owned* out) {
   for (int64_t e = 0; e < mm; ++e) g.edgesU[cur[(uint32_t)keys[e]]++] = (uint32_t)(keys[e] >> 32);  // v ascending
   *out = g;
   return PB_OK;
+}
+
+// ---- sparsification (approximate counting) -------------------------------------------------
+// Host preprocessing, like the readers: the sparsified graph is then counted on the GPU.
+namespace {
+
+// The 64-bit integer mixer of ligra/utils.h:389-397 (hashInt(ulong)).  Its constants decide which
+// edges a sparsification keeps, so they have to be the reference's for the same sample.
+inline uint64_t mix64_ligra(uint64_t a) {
+  a = (a + 0x7ed55d166bef7a1dull) + (a << 12);
+  a = (a ^ 0xc761c23c510fa2ddull) ^ (a >> 9);
+  a = (a + 0x165667b183a9c0e1ull) + (a << 59);
+  a = (a + 0xd3a2646cab3487e3ull) ^ (a << 49);
+  a = (a + 0xfd7046c5ef9ab54cull) + (a << 3);
+  a = (a ^ 0xb55a4f090dd4a67bull) ^ (a >> 32);
+  return a;
+}
+
+// Keeps the edges for which keep(v, u) holds, in list order on both sides, then drops the
+// vertices left without edges and renumbers each side in increasing order
+// (eSparseBipartite / clrSparseBipartite + delZeroDeg, butterfly_utils.h:744-996).
+template <class Keep>
+pb_status filter_graph(const pb_csr* g, Keep&& keep, pb_csr_owned* out) {
+  const int64_t nv = g->nv, nu = g->nu;
+  std::vector<uint32_t> offV(nv + 1, 0), offU(nu + 1, 0), eV, eU;
+  eV.reserve((size_t)g->m);
+  eU.reserve((size_t)g->m);
+  for (int64_t v = 0; v < nv; ++v) {
+    for (uint32_t j = g->offsetsV[v]; j < g->offsetsV[v + 1]; ++j)
+      if (keep((uint32_t)v, g->edgesV[j])) eV.push_back(g->edgesV[j]);
+    offV[v + 1] = (uint32_t)eV.size();
+  }
+  for (int64_t u = 0; u < nu; ++u) {
+    for (uint32_t j = g->offsetsU[u]; j < g->offsetsU[u + 1]; ++j)
+      if (keep(g->edgesU[j], (uint32_t)u)) eU.push_back(g->edgesU[j]);
+    offU[u + 1] = (uint32_t)eU.size();
+  }
+  if (eV.size() != eU.size()) return PB_EINVAL;  // the two sides of the input disagree
+  // New ids of the vertices that keep an edge.
+  std::vector<uint32_t> idV(nv), idU(nu);
+  int64_t kv = 0, ku = 0;
+  for (int64_t v = 0; v < nv; ++v) idV[v] = offV[v + 1] > offV[v] ? (uint32_t)kv++ : UINT32_MAX;
+  for (int64_t u = 0; u < nu; ++u) idU[u] = offU[u + 1] > offU[u] ? (uint32_t)ku++ : UINT32_MAX;
+  const int64_t m = (int64_t)eV.size();
+  std::memset(out, 0, sizeof(*out));
+  out->nv = kv;
+  out->nu = ku;
+  out->m = m;
+  out->offsetsV = (uint32_t*)std::malloc(sizeof(uint32_t) * (kv + 1));
+  out->offsetsU = (uint32_t*)std::malloc(sizeof(uint32_t) * (ku + 1));
+  out->edgesV = (uint32_t*)std::malloc(sizeof(uint32_t) * (m ? m : 1));
+  out->edgesU = (uint32_t*)std::malloc(sizeof(uint32_t) * (m ? m : 1));
+  if (!out->offsetsV || !out->offsetsU || !out->edgesV || !out->edgesU) {
+    pb_csr_free(out);
+    return PB_ENOMEM;
+  }
+  for (int64_t v = 0; v < nv; ++v)
+    if (idV[v] != UINT32_MAX) out->offsetsV[idV[v]] = offV[v];
+  out->offsetsV[kv] = (uint32_t)m;
+  for (int64_t u = 0; u < nu; ++u)
+    if (idU[u] != UINT32_MAX) out->offsetsU[idU[u]] = offU[u];
+  out->offsetsU[ku] = (uint32_t)m;
+  for (int64_t k = 0; k < m; ++k) {
+    out->edgesV[k] = idU[eV[k]];
+    out->edgesU[k] = idV[eU[k]];
+  }
+  return PB_OK;
+}
+
+}  // namespace
+
+extern "C" pb_status pb_sparsify_bipartite(const pb_csr* g, int32_t sparse_type, int64_t denom, int64_t seed,
+                                           pb_csr_owned* out) {
+  if (!g || !out) return PB_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  if (g->nv < 0 || g->nu < 0 || g->m < 0) return PB_EINVAL;
+  const uint64_t colors = denom > 1 ? (uint64_t)denom : 1u;
+  if (sparse_type == PB_SPARSE_EDGE) {
+    // eSparseBipartite (butterfly_utils.h:798-809): edge (v, u) keeps colour 0 of a hash of both
+    // ids and the seed.  v + 0x9e3779b9 is computed in 64 bits, u + 0x9e3779b9 in 32 bits (the
+    // reference's operand types), the rest in 64 bits.
+    const int64_t sh = (seed << 6) + (seed >> 2);
+    return filter_graph(g, [&](uint32_t v, uint32_t u) {
+      int64_t concat = (int64_t)v + (int64_t)0x9e3779b9u + sh;
+      concat ^= (int64_t)(uint32_t)(u + 0x9e3779b9u) + sh;
+      return mix64_ligra((uint64_t)seed + (uint64_t)concat) % colors == 0;
+    }, out);
+  }
+  if (sparse_type == PB_SPARSE_COLOR) {
+    // clrSparseBipartite (:919-925): every vertex gets a colour from its id and the seed (the same
+    // function on both sides); an edge stays when its endpoints share a colour.
+    return filter_graph(g, [&](uint32_t v, uint32_t u) {
+      return mix64_ligra((uint64_t)seed + v) % colors == mix64_ligra((uint64_t)seed + u) % colors;
+    }, out);
+  }
+  return PB_EINVAL;
+}
+
+extern "C" int64_t pb_sparse_estimate(int64_t sparse_count, int32_t sparse_type, int64_t denom) {
+  // BipartiteButterflies.C:213-214: the long count is multiplied by pow(denom, 3) (colour) or
+  // pow(denom, 4) (edge) in double precision and truncated back.
+  long long x = sparse_count;
+  if (sparse_type == PB_SPARSE_COLOR) x = (long long)((double)x * std::pow((double)denom, 3.0));
+  else if (sparse_type == PB_SPARSE_EDGE) x = (long long)((double)x * std::pow((double)denom, 4.0));
+  return (int64_t)x;
 }

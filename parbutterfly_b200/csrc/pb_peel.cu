@@ -288,18 +288,6 @@ __device__ __forceinline__ void t_put(uint32_t* keys, uint32_t* vals, uint32_t m
   atomicOr(&ctl->err, ERR_TABLE);
 }
 
-__device__ __forceinline__ bool t_get(const uint32_t* keys, const uint32_t* vals, uint32_t mask, uint32_t key,
-                                      uint32_t& val) {
-  uint32_t h = hslot(key, mask);
-  for (uint32_t probes = 0; probes <= mask; ++probes) {
-    uint32_t k = keys[h];
-    if (k == key) { val = vals[h]; return true; }
-    if (k == kEmpty) return false;
-    h = (h + 1) & mask;
-  }
-  return false;
-}
-
 // Slot of key, or kEmpty when absent.
 __device__ __forceinline__ uint32_t t_slot(const uint32_t* keys, uint32_t mask, uint32_t key) {
   uint32_t h = hslot(key, mask);
@@ -882,31 +870,7 @@ struct Classify {
   __device__ __forceinline__ bool wing_from_v(const Lists& G, uint32_t v, uint32_t u) const {
     return cost_v(G, v, u) <= cost_u(G, v, u);
   }
-  __device__ __forceinline__ bool wing_small(const Lists& G, uint32_t e) const {
-    const uint32_t v = G.center_of[e], u = G.u_of[e];
-    const bool fv = wing_from_v(G, v, u);
-    const int64_t work = fv ? cost_v(G, v, u) : cost_u(G, v, u);
-    const uint32_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
-    return work <= small_work && 2 * psize <= (uint32_t)kWarpSlots;
-  }
   __device__ __forceinline__ bool tip_huge(const Lists& G, uint32_t u) const { return G.wk[u] > huge_work; }
-  // Work units of a CTA-level wing item: first-level slices of at least max(chunk_work,
-  // 4 x probe set) estimated probes each (every unit rebuilds the probe table).
-  __device__ __forceinline__ uint32_t wing_chunks(const Lists& G, uint32_t e) const {
-    const uint32_t v = G.center_of[e], u = G.u_of[e];
-    const bool fv = wing_from_v(G, v, u);
-    const int64_t work = fv ? cost_v(G, v, u) : cost_u(G, v, u);
-    const int64_t psize = fv ? G.offK[u + 1] - G.offK[u] : G.offC[v + 1] - G.offC[v];
-    const int64_t d1 = fv ? G.offC[v + 1] - G.offC[v] : G.offK[u + 1] - G.offK[u];
-    const int64_t c = max(chunk_work, 4 * psize);
-    int64_t k = (work + c - 1) / c;
-    k = min(k, min(d1, (int64_t)4096));
-    return (uint32_t)max(k, (int64_t)1);
-  }
-  __device__ __forceinline__ bool wing_huge(const Lists& G, uint32_t e) const {
-    const uint32_t v = G.center_of[e], u = G.u_of[e];
-    return min(cost_v(G, v, u), cost_u(G, v, u)) > huge_work;
-  }
 };
 
 // Estimated work of peeling item x (plus one, so that items without work still count): the

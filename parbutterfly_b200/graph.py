@@ -165,6 +165,21 @@ class BipartiteGraph:
         _ffi.check(_ffi.lib().pb_read_konect(os.fsencode(path), C.byref(s)), what=path)
         return BipartiteGraph._from_owned(s)
 
+    def sparsify(self, sparse_type: str, denom: int = 25, seed: int = 0) -> "BipartiteGraph":
+        """Sparsified copy for approximate total counts: "EDGE" (eSparseBipartite) or "COLOR"
+        (clrSparseBipartite), denom = -d, seed 0 as in the reference's driver
+        (butterfly_utils.h:744-996).  Scale the copy's total count with sparse_estimate."""
+        s = self.csr_struct()
+        o = _ffi.CSR()
+        _ffi.check(_ffi.lib().pb_sparsify_bipartite(C.byref(s), _ffi.SPARSE[sparse_type], int(denom), int(seed),
+                                                     C.byref(o)), what="pb_sparsify_bipartite")
+        return BipartiteGraph._from_owned(o)
+
+    @staticmethod
+    def sparse_estimate(sparse_count: int, sparse_type: str, denom: int = 25) -> int:
+        """The reference's estimate from a sparsified graph's total (BipartiteButterflies.C:213-214)."""
+        return int(_ffi.lib().pb_sparse_estimate(int(sparse_count), _ffi.SPARSE[sparse_type], int(denom)))
+
     def write_binary(self, base: str) -> None:
         """hyperAdjToBinary's layout: base.config, .vidx, .vadj, .hidx, .hadj."""
         s = self.csr_struct()

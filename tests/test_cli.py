@@ -10,6 +10,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 import oracle
@@ -77,3 +78,42 @@ def test_pbb_prints_the_reference_lines(hyper, flags, per):
     ours = _run(PBB, flags, path)
     assert _lines(ours) == _lines(ref)
     assert _stages(ours) == _stages(ref)
+
+
+# Sparsification (BipartiteButterflies.C:175-193, 213-214, 333-340): long and numeric flags.
+SPARSE_SETS = [
+    (["-sparseType", "EDGE", "-d", "2"], "EDGE", 2),
+    (["-sparseType", "COLOR", "-d", "3"], "COLOR", 3),
+    (["-s", "2", "-d", "5"], "EDGE", 5),
+    (["-s", "1", "-d", "25", "-per", "VERT"], "COLOR", 25),
+]
+
+
+@needs_ref
+@pytest.mark.parametrize("flags,kind,denom", SPARSE_SETS)
+def test_reference_driver_sparse_matches_host_sparsifier(hyper, flags, kind, denom):
+    """The reference driver's estimate equals the host sparsifier's graph counted by the oracle
+    and scaled as the reference scales it: pins pb_sparsify_bipartite and pb_sparse_estimate."""
+    g, path = hyper
+    lines = _lines(_run(REF_CLI, flags, path))
+    h = g.sparsify(kind, denom)
+    est = BipartiteGraph.sparse_estimate(oracle.count(h, "TOTAL", "ADEG")[0], kind, denom)
+    assert lines == [f"number of butterflies: {est}"]
+
+
+def test_sparsify_keeps_a_valid_graph():
+    g = BipartiteGraph.zipf(300, 200, 4000, 1.3, 33)
+    for kind in ("EDGE", "COLOR"):
+        h = g.sparsify(kind, 4)
+        assert 0 < h.m < g.m
+        assert h.offsetsV[-1] == h.m and h.offsetsU[-1] == h.m
+        assert (np.diff(h.offsetsV) > 0).all() and (np.diff(h.offsetsU) > 0).all()  # no vertex without edges
+        assert h.sparsify(kind, 1).m == h.m  # one colour keeps everything
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("flags,kind,denom", SPARSE_SETS)
+def test_pbb_sparse_prints_the_reference_lines(hyper, flags, kind, denom):
+    _, path = hyper
+    assert _lines(_run(PBB, flags, path)) == _lines(_run(REF_CLI, flags, path))
