@@ -173,7 +173,8 @@ pb_status pb_graph_download(const pb_graph* g, pb_csr_owned* out);
 /* cmpWedgeCounts (butterfly_utils.h:1080-1086): *use_v = (W_V <= W_U), *num_wedges = min. */
 pb_status pb_cmp_wedge_counts(pb_ctx* ctx, const pb_graph* g, int32_t* use_v, int64_t* num_wedges);
 
-/* edgeToIdxs (butterfly_utils.h:2034-2062): eti[m], for the orientation given by use_v. */
+/* edgeToIdxs (butterfly_utils.h:2034-2062): eti[m], for the orientation given by use_v.
+ * idxsToEdge (:2065-2067) is the same call with use_v inverted. */
 pb_status pb_edge_to_idxs(pb_ctx* ctx, const pb_graph* g, int32_t use_v, uint32_t* eti);
 
 /* ---- counting -------------------------------------------------------------------------- */

@@ -5,6 +5,7 @@ calls (apps/hyper/BipartiteButterflies.C:75-277):
 
   cmp_wedge_counts(G)                -> cmpWedgeCounts   (butterfly_utils.h:1080-1086)
   edge_to_idxs(G, use_v)             -> edgeToIdxs       (butterfly_utils.h:2034-2062)
+  idxs_to_edge(G, use_v)             -> idxsToEdge       (butterfly_utils.h:2065-2067)
   count(G, count_type, rank_type)    -> Count            (butterfly_count.h:1634-1731)
   count_e(G, count_type, rank_type)  -> CountE           (butterfly_ecount.h:1766-1899)
   count_total(G, ...)                -> CountTotal       (butterfly_count_total.h:1014-1102)
@@ -207,10 +208,17 @@ def cmp_wedge_counts(dg: DeviceGraph):
 
 
 def edge_to_idxs(dg: DeviceGraph, use_v: bool):
+    """edgeToIdxs (butterfly_utils.h:2034-2062): for every edge in the use_v orientation, its
+    position in the other orientation's lists."""
     eti = np.zeros(max(dg.m, 1), dtype=np.uint32)
     dg.ctx.check(dg.ctx._lib.pb_edge_to_idxs(dg.ctx.handle, dg.handle, int(use_v), eti.ctypes.data),
                  "pb_edge_to_idxs")
     return eti[:dg.m]
+
+
+def idxs_to_edge(dg: DeviceGraph, use_v: bool):
+    """idxsToEdge (butterfly_utils.h:2065-2067): edgeToIdxs of the other orientation."""
+    return edge_to_idxs(dg, not use_v)
 
 
 def count(dg: DeviceGraph, count_type="SERIAL", rank_type="ADEG", use_v=None, out=None, **kw):
