@@ -143,6 +143,7 @@ def test_eti_matches_oracle(ctx, golden):
         dg = ctx.upload(g)
         for uv in (False, True):
             np.testing.assert_array_equal(pb.edge_to_idxs(dg, uv), oracle.edge_to_idxs(g, uv), err_msg=name)
+            np.testing.assert_array_equal(pb.idxs_to_edge(dg, uv), oracle.edge_to_idxs(g, not uv), err_msg=name)
 
 
 @pytest.mark.parametrize("smem,small_w,acc64", [("16384", "0", "0"), ("20000", "64", "1"), ("196608", "512", "1")])
