@@ -6,7 +6,10 @@ built (`make -C oracle`).  Every graph below is passed to the compiled reference
 stored.  tests/test_oracle_golden.py pins the C restatement (oracle/pb_oracle.c) to these
 vectors; the GPU tests compare against the restatement.
 
-Modes recorded (the reference paths that give correct results):
+Modes recorded: the reference paths that give correct results.  Ranked HASH/HIST per-vertex
+credits use the wrong filter (butterfly_count.h:364-367), SERIAL+SIDE+VERT writes unstrided
+results (:1371-1372), TOTAL has no branch for the A* types (butterfly_count_total.h:970-974),
+and wing peeling is only correct with PBATCHS/PBATCHWA.
   counts : BATCHS with every rank type, per VERT / EDGE / TOTAL
   tip    : PBATCHS peeling of ADEG/BATCHS per-vertex counts
   wing   : PBATCHS peeling of ADEG/BATCHS per-edge counts
